@@ -1,0 +1,392 @@
+// liblbm host engine: contexts, structure upload and bit packing, the plain
+// solve loops (one launch per step, on-device convergence controller, one
+// host synchronisation per convergence check), velocity export and the
+// diagnostic entry points.  The C ABI is declared in include/lbm.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm.h"
+#include "engine2d.cuh"
+#include "engine_host.h"
+
+using namespace lbm;
+
+// ------------------------------------------------------------- utilities ----
+int lbm_fail_cuda(lbm_ctx *ctx, cudaError_t e, const char *what, int line)
+{
+    if (ctx)
+        ctx->err = std::string("CUDA error: ") + cudaGetErrorString(e) + " in " + what +
+                   " (engine line " + std::to_string(line) + ")";
+    return LBM_ECUDA;
+}
+
+int lbm_fail_input(lbm_ctx *ctx, const std::string &msg)
+{
+    if (ctx) ctx->err = msg;
+    return LBM_EINPUT;
+}
+
+bool lbm_is_device_ptr(const void *p)
+{
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Pack a byte mask (x fastest, 1 = solid) into rows of 32-bit words, count
+// the pore voxels and flag any value other than 0/1 (LMB3d/lbm3d-perm.cpp:190-192).
+__global__ void pack_mask_kernel(const uint8_t *__restrict__ solid, int nx, long long rows, int wpr,
+                                 uint32_t *__restrict__ mask, unsigned long long *npore, unsigned *bad)
+{
+    const long long total = rows * wpr;
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
+         w += (long long)gridDim.x * blockDim.x) {
+        const long long r = w / wpr;
+        const int c = (int)(w - r * wpr);
+        const int x0 = c * 32;
+        const uint8_t *row = solid + r * nx;
+        uint32_t bits = 0;
+        unsigned cnt = 0, b = 0;
+        for (int i = 0; i < 32 && x0 + i < nx; ++i) {
+            const uint8_t v = row[x0 + i];
+            b |= v > 1;
+            if (v) bits |= 1u << i; else ++cnt;
+        }
+        mask[w] = bits;
+        if (cnt) atomicAdd(npore, (unsigned long long)cnt);
+        if (b) atomicOr(bad, 1u);
+    }
+}
+
+int lbm_upload_mask(lbm_ctx *ctx, const uint8_t *solid, int nx, long long rows, DevMem &mask,
+                    long long &npore)
+{
+    const long long nn = (long long)nx * rows;
+    const int wpr = (nx + 31) / 32;
+    DevMem staging(ctx->stream), scratch(ctx->stream);
+    const uint8_t *src = solid;
+    if (!lbm_is_device_ptr(solid)) {
+        CK(staging.alloc((size_t)nn));
+        CK(cudaMemcpyAsync(staging.p, solid, (size_t)nn, cudaMemcpyHostToDevice, ctx->stream));
+        src = static_cast<const uint8_t *>(staging.p);
+    }
+    CK(mask.alloc(sizeof(uint32_t) * (size_t)rows * wpr));
+    CK(scratch.alloc(16));
+    CK(cudaMemsetAsync(scratch.p, 0, 16, ctx->stream));
+    auto *cnt = static_cast<unsigned long long *>(scratch.p);
+    auto *bad = reinterpret_cast<unsigned *>(cnt + 1);
+    const long long words = rows * wpr;
+    const int blocks = (int)std::min<long long>((words + 255) / 256, 4L * 1184);
+    pack_mask_kernel<<<blocks, 256, 0, ctx->stream>>>(src, nx, rows, wpr, static_cast<uint32_t *>(mask.p), cnt, bad);
+    CK(cudaGetLastError());
+    unsigned long long h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, scratch.p, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if ((unsigned)h[1]) return lbm_fail_input(ctx, "non-binary voxel");
+    npore = (long long)h[0];
+    if (npore == 0) return lbm_fail_input(ctx, "structure has no pore space");
+    return LBM_OK;
+}
+
+// ------------------------------------------------------------- context ------
+extern "C" int lbm_version(void) { return LBM_API_VERSION; }
+
+extern "C" int lbm_create(lbm_ctx **out, int device)
+{
+    if (!out) return LBM_EINPUT;
+    *out = nullptr;
+    lbm_ctx *ctx = new lbm_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        lbm_last_error_global() = std::string("CUDA error: ") + cudaGetErrorString(e);
+        delete ctx;
+        return LBM_ECUDA;
+    }
+    *out = ctx;
+    return LBM_OK;
+}
+
+extern "C" void lbm_destroy(lbm_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+std::string &lbm_last_error_global()
+{
+    static std::string s;
+    return s;
+}
+
+extern "C" const char *lbm_last_error(const lbm_ctx *ctx)
+{
+    return ctx ? ctx->err.c_str() : lbm_last_error_global().c_str();
+}
+
+// --------------------------------------------------------------- 3D ---------
+int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
+{
+    if (!(p.tau > 0.5)) return lbm_fail_input(ctx, "tau must exceed 0.5");
+    if (p.lag <= 0) return lbm_fail_input(ctx, "--lag must be positive");
+    if (p.precision < LBM_FP64 || p.precision > LBM_BF16) return lbm_fail_input(ctx, "unknown precision");
+    if (p.criterion != LBM_CRIT_DRIFT && p.criterion != LBM_CRIT_BLOCK) return lbm_fail_input(ctx, "unknown criterion");
+    if (p.criterion == LBM_CRIT_BLOCK && (p.sample <= 0 || p.lag % p.sample != 0))
+        return lbm_fail_input(ctx, "block criterion needs sample > 0 dividing lag");
+    if (p.npt != 0 && p.npt != 1 && p.npt != 2 && !(p.npt == 4 && p.precision != LBM_FP64))
+        return lbm_fail_input(ctx, "npt must be 1, 2 or 4 (1 or 2 for FP64)");
+    return LBM_OK;
+}
+
+static size_t elem_size(int prec) { return prec == LBM_FP64 ? 8 : (prec == LBM_FP32 ? 4 : 2); }
+
+long long lbm_plane_elems(long long nn) { return (nn + 63) / 64 * 64; }
+
+long long lbm_lattice_bytes3d(long long nn, int prec)
+{
+    return (long long)Q3 * lbm_plane_elems(nn) * (long long)elem_size(prec);
+}
+
+void lbm_fill_solve3(Solve3 &S, int nx, int ny, int nz, const double F[3], const lbm_params3d &p, int npt)
+{
+    memset(&S, 0, sizeof(S));
+    S.nx = nx; S.ny = ny; S.nz = nz;
+    S.wpr = (nx + 31) / 32;
+    S.nn = (long long)nx * ny * nz;
+    S.plane = lbm_plane_elems(S.nn);
+    S.ntiles = (int)((S.nn + TPB * npt - 1) / (TPB * npt));
+    S.dvx.init(nx);
+    S.dvy.init(ny);
+    Phys3 &P = S.P;
+    for (int c = 0; c < 3; ++c) { P.F[c] = F[c]; P.Ff[c] = (float)F[c]; }
+    P.tau = p.tau;
+    P.pref = 1.0 - 0.5 / p.tau;
+    P.omega = (float)(1.0 / p.tau);
+    P.preff = (float)P.pref;
+    // FP16 keeps h * scale; scale puts the largest plausible deviation
+    // (Poiseuille peak |F| L^2 / 8 nu over the longest axis) near 2^12, far
+    // from both the overflow at 65504 and the subnormal range.
+    double scale = 1.0;
+    if (p.precision == LBM_FP16) {
+        const double nu = (p.tau - 0.5) / 3.0;
+        const double L = (double)std::max(nx, std::max(ny, nz));
+        const double fmag = std::sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]);
+        const double uest = fmag * L * L / (8.0 * nu);
+        scale = uest > 0 ? std::exp2(std::round(std::log2(4096.0 / uest))) : 1.0;
+        scale = std::min(std::max(scale, 1.0), std::exp2(40.0));
+    }
+    S.scale = (float)scale;
+    S.inv_scale = (float)(1.0 / scale);
+    Ctl3 &c = S.c;
+    c.eps = p.eps; c.lag = p.lag; c.min_steps = p.min_steps; c.max_steps = p.max_steps;
+    c.avg_steps = p.avg_steps; c.hold = p.hold; c.criterion = p.criterion;
+    c.sample = p.sample > 0 ? p.sample : 1; c.ksigma = p.ksigma;
+}
+
+void lbm_init_state3(State3 &st, const Ctl3 &c)
+{
+    memset(&st, 0, sizeof(st));
+    st.phase = PH_RUN;
+    if (c.max_steps <= 0) {
+        // no run-in steps: converged iff hold <= 0 (LMB3d/lbm3d-perm.cpp:362)
+        st.converged = 0 >= c.hold ? 1 : 0;
+        if (c.avg_steps <= 0) { st.phase = PH_DONE; st.steps = 0; }
+        else { st.phase = PH_AVG; st.avg_start = 0; }
+    }
+}
+
+int lbm_pick_npt(const lbm_params3d &p) { return p.npt > 0 ? p.npt : 1; }
+
+// Run a set of 3D solves sharing one mask to completion, one launch per step.
+// The host synchronises only where the controller can change phase: on lag
+// multiples and max_steps in phase 1, at the end of the averaging phase.
+static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, State3 *d_states,
+                       const int2 *d_work, int nwork, int prec, int npt, std::vector<State3> &hst)
+{
+    const int n = (int)hs.size();
+    long long s = 0;
+    StepArgs a;
+    a.solves = d_solves; a.work = d_work; a.nwork_dev = nullptr; a.nwork = nwork;
+    for (;;) {
+        CK(cudaMemcpyAsync(hst.data(), d_states, sizeof(State3) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        long long target = LLONG_MAX;
+        for (int j = 0; j < n; ++j) {
+            const State3 &st = hst[j];
+            const Ctl3 &c = hs[j].c;
+            if (st.phase == PH_RUN) {
+                long long nx = (s / c.lag + 1) * c.lag;
+                if (c.max_steps > s) nx = std::min(nx, c.max_steps);
+                target = std::min(target, nx);
+            } else if (st.phase == PH_AVG) {
+                target = std::min(target, st.avg_start + c.avg_steps);
+            }
+        }
+        if (target == LLONG_MAX) break;
+        for (; s < target; ++s) {
+            a.step = s;
+            cudaError_t e = prec == LBM_FP64 ? launch_step3d_f64(npt, dim3(nwork), ctx->stream, a)
+                                             : launch_step3d_lp(prec, npt, dim3(nwork), ctx->stream, a);
+            CK(e);
+        }
+    }
+    return LBM_OK;
+}
+
+extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz,
+                           int ndir, const double *forces, const lbm_params3d *params,
+                           lbm_result3d *results, float *vel_out)
+{
+    if (!ctx) return LBM_EINPUT;
+    if (!solid || !forces || !params || !results || ndir <= 0)
+        return lbm_fail_input(ctx, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    if (nx <= 0 || ny <= 0 || nz <= 0) return lbm_fail_input(ctx, "bad dimensions");
+    const long long nn = (long long)nx * ny * nz;
+    if (nn >= (1ll << 31) || (long long)Q3 * lbm_plane_elems(nn) >= (1ll << 32))
+        return lbm_fail_input(ctx, "lattice too large (19 x nodes must stay below 2^32)");
+    const lbm_params3d p = *params;
+    int rc = lbm_check_params3d(ctx, p);
+    if (rc) return rc;
+    const int prec = p.precision, npt = lbm_pick_npt(p);
+
+    DevMem mask(ctx->stream);
+    long long npore = 0;
+    rc = lbm_upload_mask(ctx, solid, nx, (long long)ny * nz, mask, npore);
+    if (rc) return rc;
+
+    std::vector<Solve3> hs(ndir);
+    std::vector<State3> hst(ndir);
+    std::vector<DevMem> lat, part;
+    lat.reserve(ndir); part.reserve(ndir);
+    DevMem d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream);
+    CK(d_states.alloc(sizeof(State3) * ndir));
+    for (int j = 0; j < ndir; ++j) {
+        Solve3 &S = hs[j];
+        lbm_fill_solve3(S, nx, ny, nz, forces + 3 * j, p, npt);
+        lat.emplace_back(ctx->stream);
+        part.emplace_back(ctx->stream);
+        CK(lat.back().alloc((size_t)lbm_lattice_bytes3d(nn, prec)));
+        CK(part.back().alloc(sizeof(double) * 3 * (size_t)S.ntiles));
+        S.A = lat.back().p;
+        S.mask = static_cast<const uint32_t *>(mask.p);
+        S.partials = static_cast<double *>(part.back().p);
+        S.st = static_cast<State3 *>(d_states.p) + j;
+        lbm_init_state3(hst[j], S.c);
+        CK(launch_init3d(prec, S.A, S.plane, S.nn, ctx->stream));
+    }
+    std::vector<int2> work;
+    for (int j = 0; j < ndir; ++j)
+        for (int t = 0; t < hs[j].ntiles; ++t) work.push_back(make_int2(j, t));
+    CK(d_solves.alloc(sizeof(Solve3) * ndir));
+    CK(d_work.alloc(sizeof(int2) * work.size()));
+    CK(cudaMemcpyAsync(d_solves.p, hs.data(), sizeof(Solve3) * ndir, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_work.p, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_states.p, hst.data(), sizeof(State3) * ndir, cudaMemcpyHostToDevice, ctx->stream));
+
+    rc = run_plain3d(ctx, hs, static_cast<Solve3 *>(d_solves.p), static_cast<State3 *>(d_states.p),
+                     static_cast<const int2 *>(d_work.p), (int)work.size(), prec, npt, hst);
+    if (rc) return rc;
+
+    if (vel_out) {
+        const bool dev = lbm_is_device_ptr(vel_out);
+        DevMem vbuf(ctx->stream);
+        if (!dev) CK(vbuf.alloc(sizeof(float) * 3 * (size_t)nn));
+        for (int j = 0; j < ndir; ++j) {
+            float *dst = dev ? vel_out + 3 * nn * j : static_cast<float *>(vbuf.p);
+            CK(launch_canon3d(prec, hs[j], hst[j].steps, nullptr, dst, ctx->stream));
+            if (!dev)
+                CK(cudaMemcpyAsync(vel_out + 3 * nn * j, vbuf.p, sizeof(float) * 3 * nn,
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+
+    int out = LBM_OK;
+    for (int j = 0; j < ndir; ++j) {
+        const State3 &st = hst[j];
+        lbm_result3d &r = results[j];
+        for (int c = 0; c < 3; ++c) { r.q[c] = st.q[c]; r.se[c] = st.se[c]; }
+        r.steps = st.steps;
+        r.converged = st.converged;
+        r.status = st.status;
+        if (st.status) {
+            ctx->err = "non-finite flux in run " + std::to_string(j) + " at step " + std::to_string(st.steps);
+            out = LBM_EINPUT;
+        } else if (!st.converged && out == LBM_OK) {
+            out = LBM_NOT_CONVERGED;
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return out;
+}
+
+extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz,
+                                 const double force[3], double tau, int precision, int npt,
+                                 long long nsteps, double *f_out, float *u_out, double q_out[3])
+{
+    if (!ctx) return LBM_EINPUT;
+    CK(cudaSetDevice(ctx->device));
+    if (nx <= 0 || ny <= 0 || nz <= 0) return lbm_fail_input(ctx, "bad dimensions");
+    const long long nn = (long long)nx * ny * nz;
+    if (nn >= (1ll << 31) || (long long)Q3 * lbm_plane_elems(nn) >= (1ll << 32))
+        return lbm_fail_input(ctx, "lattice too large");
+    lbm_params3d p;
+    memset(&p, 0, sizeof(p));
+    p.tau = tau; p.eps = 0.0; p.lag = LLONG_MAX / 4; p.hold = 1 << 30;
+    p.min_steps = 0; p.max_steps = nsteps; p.avg_steps = 0;
+    p.precision = precision; p.criterion = LBM_CRIT_DRIFT; p.npt = npt; p.sample = 1;
+    int rc = lbm_check_params3d(ctx, p);
+    if (rc) return rc;
+    npt = lbm_pick_npt(p);
+    DevMem mask(ctx->stream);
+    long long npore = 0;
+    rc = lbm_upload_mask(ctx, solid, nx, (long long)ny * nz, mask, npore);
+    if (rc) return rc;
+    std::vector<Solve3> hs(1);
+    std::vector<State3> hst(1);
+    Solve3 &S = hs[0];
+    lbm_fill_solve3(S, nx, ny, nz, force, p, npt);
+    DevMem lat(ctx->stream), part(ctx->stream), d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream);
+    CK(lat.alloc((size_t)lbm_lattice_bytes3d(nn, precision)));
+    CK(part.alloc(sizeof(double) * 3 * (size_t)S.ntiles));
+    CK(d_states.alloc(sizeof(State3)));
+    S.A = lat.p; S.mask = static_cast<const uint32_t *>(mask.p);
+    S.partials = static_cast<double *>(part.p); S.st = static_cast<State3 *>(d_states.p);
+    lbm_init_state3(hst[0], S.c);
+    CK(launch_init3d(precision, S.A, S.plane, S.nn, ctx->stream));
+    std::vector<int2> work;
+    for (int t = 0; t < S.ntiles; ++t) work.push_back(make_int2(0, t));
+    CK(d_solves.alloc(sizeof(Solve3)));
+    CK(d_work.alloc(sizeof(int2) * work.size()));
+    CK(cudaMemcpyAsync(d_solves.p, &S, sizeof(Solve3), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_work.p, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_states.p, hst.data(), sizeof(State3), cudaMemcpyHostToDevice, ctx->stream));
+    rc = run_plain3d(ctx, hs, static_cast<Solve3 *>(d_solves.p), static_cast<State3 *>(d_states.p),
+                     static_cast<const int2 *>(d_work.p), (int)work.size(), precision, npt, hst);
+    if (rc) return rc;
+    DevMem fb(ctx->stream), ub(ctx->stream);
+    if (f_out) CK(fb.alloc(sizeof(double) * Q3 * (size_t)nn));
+    if (u_out) CK(ub.alloc(sizeof(float) * 3 * (size_t)nn));
+    CK(launch_canon3d(precision, S, nsteps, static_cast<double *>(fb.p), static_cast<float *>(ub.p), ctx->stream));
+    if (f_out) CK(cudaMemcpyAsync(f_out, fb.p, sizeof(double) * Q3 * nn, cudaMemcpyDeviceToHost, ctx->stream));
+    if (u_out) CK(cudaMemcpyAsync(u_out, ub.p, sizeof(float) * 3 * nn, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (q_out) for (int c = 0; c < 3; ++c) q_out[c] = hst[0].q[c];
+    return LBM_OK;
+}

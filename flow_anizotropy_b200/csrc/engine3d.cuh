@@ -1,0 +1,480 @@
+// D3Q19 permeability solve on the device: data layout, the AA-pattern
+// stream-collide kernel with its fused flux reduction, and the convergence
+// controller that replaces the host loop of LMB3d/lbm3d-perm.cpp:320-398.
+//
+// Layout in HBM (one lattice per forcing direction):
+//   A[k][n]   19 planes, structure of arrays, n = (z*ny + y)*nx + x, plane
+//             stride padded to 128 B.  A single in-place buffer: the AA access
+//             pattern (Bailey et al. 2009) alternates
+//               odd steps  (local):     read A[k][n],        write A[opp k][n]
+//               even steps (neighbour): read A[opp k][n-e_k], write A[k][n+e_k]
+//             so each location is read and then rewritten by the same thread
+//             and a step needs no second buffer.  Halfway bounce-back folds
+//             into the neighbour step: a link whose far end is solid reads
+//             A[k][n] and writes A[opp k][n] instead.  Step 1 of a solve is a
+//             local step on the initial state, which is exactly the reference's
+//             collide_only priming (LMB3d/lbm3d-perm.cpp:249-253,291-295).
+//   mask      1 bit per voxel, 1 = solid, rows of ceil(nx/32) words.
+//   partials  one double3 per tile, written only on reduction steps.
+//
+// Work is a list of (solve, tile) items; a tile is TPB*NPT consecutive nodes
+// of one lattice.  One launch advances every listed solve by one step, each at
+// its own step number, so solves admitted at different times share a launch.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "d3q19.cuh"
+
+namespace lbm {
+
+constexpr int TPB = 256;     // threads per block of the step kernels
+
+// Unsigned division by a runtime constant via multiply-high (valid for
+// dividends < 2^31): q = umulhi(n, m) >> s.
+struct FastDiv {
+    int d;
+    unsigned m;
+    unsigned s;
+    void init(int div)
+    {
+        d = div;
+        if (div == 1) { m = 0; s = 0; return; }
+        unsigned l = 0;
+        while ((1u << l) < (unsigned)div) ++l;          // ceil(log2 d)
+        const unsigned long long p = 31ull + l;
+        m = (unsigned)(((1ull << p) + (unsigned)div - 1) / (unsigned)div);
+        s = (unsigned)(p - 32);
+    }
+    __device__ __forceinline__ int div(int n) const
+    {
+        return d == 1 ? n : (int)(__umulhi((unsigned)n, m) >> s);
+    }
+};
+
+// Convergence controller parameters (LMB3d/lbm3d-perm.cpp:118-130), plus the
+// optional block-mean criterion of the 2D reference (LMB2d/main.cpp:99-178)
+// for reduced-precision storage.
+struct Ctl3 {
+    double eps;
+    long long lag, min_steps, max_steps, avg_steps;
+    int hold;
+    int criterion;        // 0: instantaneous drift (reference); 1: block means
+    long long sample;     // criterion 1: flux sample interval
+    double ksigma;        // criterion 1: k-sigma acceptance
+};
+
+enum { PH_RUN = 1, PH_AVG = 2, PH_DONE = 3, PH_ERR = 4 };
+
+// Mutable per-solve state, device resident, written only by the controller.
+struct State3 {
+    long long s_base;     // steps completed before the current launch chunk
+    int phase;
+    int hold, have_prev;
+    int converged, status;
+    unsigned counter;     // tiles finished on the current reduction step
+    double qprev[3];
+    double bs[3], bss[3], pse[3];
+    long long bn;
+    double sum[3], sumsq[3];
+    long long n_avg;
+    double q[3], se[3];
+    long long steps;
+    double qlast[3];
+    long long avg_start;  // step at which phase 1 ended
+};
+
+struct Solve3 {
+    void *A;
+    long long plane;      // elements per plane
+    const uint32_t *mask;
+    int nx, ny, nz, wpr;
+    long long nn;
+    int ntiles;
+    FastDiv dvx, dvy;
+    float scale, inv_scale;
+    Phys3 P;
+    Ctl3 c;
+    double *partials;     // ntiles * 3
+    State3 *st;
+};
+
+struct StepArgs {
+    const Solve3 *solves;
+    const int2 *work;     // (solve index, tile index)
+    const int *nwork_dev; // if non-null, the item count is read here
+    int nwork;
+    long long step;       // steps completed = st->s_base + step
+};
+
+// ----------------------------------------------------------------- helpers --
+__device__ __forceinline__ int mbit(const uint32_t *row, int x)
+{
+    return (int)((__ldg(row + (x >> 5)) >> (x & 31)) & 1u);
+}
+
+__device__ __forceinline__ bool needs_reduction(const Ctl3 &c, int phase, long long n)
+{
+    if (phase == PH_AVG) return true;
+    if (n == c.max_steps) return true;
+    if (n % c.lag == 0) return true;
+    return c.criterion == 1 && (n % c.sample == 0);
+}
+
+// Controller step, run by one thread once the flux q of step n is known.
+// Phase 1 is LMB3d/lbm3d-perm.cpp:332-364 (criterion 0), or the block-mean
+// test of LMB2d/main.cpp:123-178 on 3D flux vectors (criterion 1); phase 2 is
+// the averaging of :370-390.
+__device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const double q[3])
+{
+    if (st.phase == PH_RUN) {
+        st.qlast[0] = q[0]; st.qlast[1] = q[1]; st.qlast[2] = q[2];
+        if (c.criterion == 0) {
+            if (n % c.lag == 0) {
+                for (int k = 0; k < 3; ++k)
+                    if (!isfinite(q[k])) { st.status = 2; st.phase = PH_ERR; st.steps = n; return; }
+                const double norm = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                double drift = 0.0;
+                for (int k = 0; k < 3; ++k) drift = fmax(drift, fabs(q[k] - st.qprev[k]));
+                if (st.have_prev && n >= c.min_steps && drift < c.eps * norm) st.hold++;
+                else st.hold = 0;
+                for (int k = 0; k < 3; ++k) st.qprev[k] = q[k];
+                st.have_prev = 1;
+            }
+        } else {
+            if (n % c.sample == 0) {
+                for (int k = 0; k < 3; ++k)
+                    if (!isfinite(q[k])) { st.status = 2; st.phase = PH_ERR; st.steps = n; return; }
+                for (int k = 0; k < 3; ++k) { st.bs[k] += q[k]; st.bss[k] += q[k] * q[k]; }
+                st.bn++;
+            }
+            if (n % c.lag == 0 && st.bn >= 2) {
+                const double bn = (double)st.bn;
+                double m[3], se[3];
+                for (int k = 0; k < 3; ++k) {
+                    m[k] = st.bs[k] / bn;
+                    const double v = (st.bss[k] - bn * m[k] * m[k]) / (bn - 1.0);
+                    se[k] = sqrt(fmax(v, 0.0) / bn);
+                }
+                if (st.have_prev) {
+                    const double norm = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+                    bool pass = n >= c.min_steps;
+                    for (int k = 0; k < 3; ++k) {
+                        const double tol = fmax(c.eps * norm,
+                                                c.ksigma * sqrt(se[k] * se[k] + st.pse[k] * st.pse[k]));
+                        pass = pass && fabs(m[k] - st.qprev[k]) < tol;
+                    }
+                    if (pass) st.hold++; else st.hold = 0;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    st.qprev[k] = m[k]; st.pse[k] = se[k];
+                    st.bs[k] = 0.0; st.bss[k] = 0.0;
+                }
+                st.bn = 0;
+                st.have_prev = 1;
+            }
+        }
+        const bool conv = st.hold >= c.hold;
+        if (conv || n >= c.max_steps) {
+            st.converged = conv ? 1 : 0;
+            if (c.avg_steps <= 0) {
+                for (int k = 0; k < 3; ++k) { st.q[k] = q[k]; st.se[k] = 0.0; }
+                st.steps = n;
+                st.phase = PH_DONE;
+            } else {
+                st.phase = PH_AVG;
+                st.avg_start = n;
+            }
+        }
+        return;
+    }
+    if (st.phase == PH_AVG) {
+        for (int k = 0; k < 3; ++k) { st.sum[k] += q[k]; st.sumsq[k] += q[k] * q[k]; }
+        st.n_avg++;
+        if (st.n_avg >= c.avg_steps) {
+            const double nn = (double)st.n_avg;
+            for (int k = 0; k < 3; ++k) {
+                st.q[k] = st.sum[k] / nn;
+                st.se[k] = 0.0;
+                if (st.n_avg > 1) {
+                    const double var = (st.sumsq[k] - nn * st.q[k] * st.q[k]) / (nn - 1.0);
+                    st.se[k] = sqrt(fmax(var, 0.0) / nn);
+                }
+            }
+            st.steps = n;
+            st.phase = PH_DONE;
+        }
+    }
+}
+
+// Block-wide fixed-order sum of three doubles; result valid in thread 0.
+__device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { sh[wid][0] = v[0]; sh[wid][1] = v[1]; sh[wid][2] = v[2]; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int w = 0; w < TPB / 32; ++w) { a0 += sh[w][0]; a1 += sh[w][1]; a2 += sh[w][2]; }
+        v[0] = a0; v[1] = a1; v[2] = a2;
+    }
+    __syncthreads();
+}
+
+// Tile finished on a reduction step: publish the tile's flux partial; the
+// last tile of the solve to finish sums all partials in a fixed order (the
+// result does not depend on which blocks ran which tiles, or on what else is
+// in the batch) and runs the controller.
+__device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long n,
+                                            double (&acc)[3], double (*sh)[3])
+{
+    __shared__ int s_last;
+    block_sum3(acc, sh);
+    if (threadIdx.x == 0) {
+        double *p = S.partials + 3ll * tile;
+        p[0] = acc[0]; p[1] = acc[1]; p[2] = acc[2];
+        __threadfence();
+        const unsigned prev = atomicAdd(&S.st->counter, 1u);
+        s_last = (prev == (unsigned)S.ntiles - 1u);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int t = threadIdx.x; t < S.ntiles; t += TPB) {
+        v[0] += __ldcg(S.partials + 3ll * t);
+        v[1] += __ldcg(S.partials + 3ll * t + 1);
+        v[2] += __ldcg(S.partials + 3ll * t + 2);
+    }
+    block_sum3(v, sh);
+    if (threadIdx.x == 0) {
+        State3 &st = *S.st;
+        st.counter = 0u;
+        const double inv = (double)S.nn;
+        const double q[3] = {v[0] / inv, v[1] / inv, v[2] / inv};
+        controller3(S.c, st, n, q);
+    }
+}
+
+// Neighbourhood of one node: wrapped coordinates as offsets, so the linear
+// index of x + e_k is Zb[ez+1] + Yb[ey+1] + X[ex+1], and the solid bits of
+// the 18 neighbours (bit k set if x + e_k is solid; bit 0 = the node itself).
+struct Nbr3 {
+    int X[3];             // x-1, x, x+1 (wrapped)
+    int Yb[3];            // (y-1, y, y+1) * nx
+    int Zb[3];            // (z-1, z, z+1) * nx * ny
+    uint32_t solid;
+    __device__ __forceinline__ int idx(int k) const
+    {
+        return Zb[ez3(k) + 1] + Yb[ey3(k) + 1] + X[ex3(k) + 1];
+    }
+};
+
+// Bits of one mask row at x-1, x, x+1 (bit 0, 1, 2).  The word holding x
+// usually holds both neighbours; the two others are read only at word edges
+// and at the periodic wrap.
+__device__ __forceinline__ uint32_t row3(const uint32_t *__restrict__ row, int x, int xm, int xp)
+{
+    const uint32_t w = __ldg(row + (x >> 5));
+    const int b = x & 31;
+    const uint32_t c = (w >> b) & 1u;
+    const uint32_t m = (b != 0 && xm == x - 1) ? (w >> (b - 1)) & 1u : (uint32_t)mbit(row, xm);
+    const uint32_t p = (b != 31 && xp == x + 1) ? (w >> (b + 1)) & 1u : (uint32_t)mbit(row, xp);
+    return m | (c << 1) | (p << 2);
+}
+
+__host__ __device__ constexpr int k_of(int dx, int dy, int dz)
+{
+    for (int k = 0; k < Q3; ++k)
+        if (ex3(k) == dx && ey3(k) == dy && ez3(k) == dz) return k;
+    return -1;
+}
+
+__device__ __forceinline__ void neighbours3(const Solve3 &S, int x, int y, int z, Nbr3 &nb)
+{
+    const int nx = S.nx, ny = S.ny, nz = S.nz;
+    const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+    const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
+    nb.X[0] = xm; nb.X[1] = x; nb.X[2] = xp;
+    nb.Yb[0] = ym * nx; nb.Yb[1] = y * nx; nb.Yb[2] = yp * nx;
+    const int zr[3] = {zm * ny, z * ny, zp * ny};
+    const int yr[3] = {ym, y, yp};
+    nb.Zb[0] = zr[0] * nx; nb.Zb[1] = zr[1] * nx; nb.Zb[2] = zr[2] * nx;
+    uint32_t bits = 0;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+            if (dy != 0 && dz != 0) {
+                // edge rows: only the x column is a D3Q19 neighbour
+                const uint32_t *row = S.mask + (size_t)(zr[dz + 1] + yr[dy + 1]) * S.wpr;
+                bits |= (uint32_t)mbit(row, x) << k_of(0, dy, dz);
+            } else {
+                const uint32_t *row = S.mask + (size_t)(zr[dz + 1] + yr[dy + 1]) * S.wpr;
+                const uint32_t b3 = row3(row, x, xm, xp);
+                bits |= ((b3 >> 1) & 1u) << k_of(0, dy, dz);
+                bits |= (b3 & 1u) << k_of(-1, dy, dz);
+                bits |= ((b3 >> 2) & 1u) << k_of(1, dy, dz);
+            }
+        }
+    nb.solid = bits;
+}
+
+// ----------------------------------------------------------- step kernel --
+// Resident blocks per SM the register allocation is sized for: enough
+// threads that roughly 40 KB of population loads are in flight per SM.
+template <class ST> struct MinBlocks { static constexpr int value = 2; };
+template <> struct MinBlocks<StoreF64> { static constexpr int value = 1; };
+template <> struct MinBlocks<StoreF32> { static constexpr int value = 2; };
+
+template <class ST, int NPT>
+__global__ void __launch_bounds__(TPB, MinBlocks<ST>::value) step3d_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    using Cp = typename ST::C;
+    __shared__ double sh[TPB / 32][3];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S = a.solves[item.x];
+        const int phase = S.st->phase;
+        if (phase >= PH_DONE) continue;
+        const long long n = S.st->s_base + a.step + 1;          // this step's number
+        const bool neighbour = (n & 1ll) == 0;
+        const bool red = needs_reduction(S.c, phase, n);
+        T *__restrict__ A = static_cast<T *>(S.A);
+        const unsigned P = (unsigned)S.plane;        // 19 * plane < 2^32 (checked on the host)
+        const float sc = S.scale, isc = S.inv_scale;
+        double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < NPT; ++j) {
+            const long long node = (long long)item.y * (TPB * NPT) + j * TPB + threadIdx.x;
+            if (node >= S.nn) continue;
+            const int nd = (int)node;
+            const int r = S.dvx.div(nd);
+            const int x = nd - r * S.nx;
+            if (!neighbour) {
+                if (mbit(S.mask + (size_t)r * S.wpr, x)) continue;
+                Cp g[Q3];
+#pragma unroll
+                for (int k = 0; k < Q3; ++k) g[k] = ST::ld(A + (k * P + (unsigned)nd), isc);
+                Cp ux, uy, uz;
+                if constexpr (ST::shifted) collide_shift32(g, S.P, ux, uy, uz);
+                else collide_ref64(g, S.P, ux, uy, uz);
+#pragma unroll
+                for (int k = 0; k < Q3; ++k) ST::st(A + (opp3(k) * P + (unsigned)nd), g[k], sc);
+                acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+            } else {
+                const int z = S.dvy.div(r);
+                const int y = r - z * S.ny;
+                Nbr3 nb;
+                neighbours3(S, x, y, z, nb);
+                if (nb.solid & 1u) continue;
+                Cp g[Q3];
+                g[0] = ST::ld(A + nd, isc);
+#pragma unroll
+                for (int k = 1; k < Q3; ++k) {
+                    // pull from x - e_k = x + e_opp(k); bounce back if it is solid
+                    const int o = opp3(k);
+                    g[k] = ((nb.solid >> o) & 1u) ? ST::ld(A + (k * P + (unsigned)nd), isc)
+                                                  : ST::ld(A + (o * P + (unsigned)nb.idx(o)), isc);
+                }
+                Cp ux, uy, uz;
+                if constexpr (ST::shifted) collide_shift32(g, S.P, ux, uy, uz);
+                else collide_ref64(g, S.P, ux, uy, uz);
+                ST::st(A + nd, g[0], sc);
+#pragma unroll
+                for (int k = 1; k < Q3; ++k) {
+                    if ((nb.solid >> k) & 1u) ST::st(A + (opp3(k) * P + (unsigned)nd), g[k], sc);
+                    else ST::st(A + (k * P + (unsigned)nb.idx(k)), g[k], sc);
+                }
+                acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+            }
+        }
+        if (red) finish_tile(S, item.y, n, acc, sh);
+    }
+}
+
+// After a chunk of `steps` launches, solves still running have advanced by it.
+__global__ void advance3d_kernel(Solve3 *solves, int nsolves, long long steps);
+
+// Initial state: every population at rest (f = w, or h = 0 when shifted).
+template <class ST>
+__global__ void init3d_kernel(void *A, long long plane, long long nn)
+{
+    using T = typename ST::T;
+    T *a = static_cast<T *>(A);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
+         i += (long long)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < Q3; ++k) {
+            if constexpr (ST::shifted) a[k * plane + i] = T(0.0f);
+            else a[k * plane + i] = (T)ST::init(k);
+        }
+}
+
+// Post-collision populations f*_k(x) of the last completed step `done`
+// (canonical, as the reference's f0 holds them), and/or the velocity of that
+// step recovered from them: Guo forcing gives j* = j + F, so
+// u = (j* - F/2) / rho.  Solid nodes get u = 0 and f = 0.
+template <class ST>
+__global__ void canon3d_kernel(const Solve3 S, long long done, double *f_out, float *u_out)
+{
+    using T = typename ST::T;
+    const T *A = static_cast<const T *>(S.A);
+    const long long P = S.plane;
+    for (long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x; node < S.nn;
+         node += (long long)gridDim.x * blockDim.x) {
+        const int nd = (int)node;
+        const int r = S.dvx.div(nd);
+        const int x = nd - r * S.nx;
+        const int z = S.dvy.div(r);
+        const int y = r - z * S.ny;
+        Nbr3 nb;
+        neighbours3(S, x, y, z, nb);
+        if (nb.solid & 1u) {
+            if (f_out) for (int k = 0; k < Q3; ++k) f_out[node * Q3 + k] = 0.0;
+            if (u_out) { u_out[3 * node] = 0.f; u_out[3 * node + 1] = 0.f; u_out[3 * node + 2] = 0.f; }
+            continue;
+        }
+        double f[Q3];
+#pragma unroll
+        for (int k = 0; k < Q3; ++k) {
+            const int o = opp3(k);
+            double v;
+            if (done == 0) v = (double)ST::ld(A + k * P + nd, S.inv_scale);          // initial, pre-collision
+            else if (done & 1ll) v = (double)ST::ld(A + o * P + nd, S.inv_scale);     // after a local step
+            else if (k == 0) v = (double)ST::ld(A + nd, S.inv_scale);
+            else if ((nb.solid >> k) & 1u) v = (double)ST::ld(A + o * P + nd, S.inv_scale);
+            else v = (double)ST::ld(A + k * P + nb.idx(k), S.inv_scale);
+            f[k] = ST::shifted ? v + w3(k) : v;
+        }
+        if (f_out)
+            for (int k = 0; k < Q3; ++k) f_out[node * Q3 + k] = f[k];
+        if (u_out) {
+            double rho = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
+            for (int k = 0; k < Q3; ++k) {
+                rho += f[k]; jx += f[k] * ex3(k); jy += f[k] * ey3(k); jz += f[k] * ez3(k);
+            }
+            const double sh = done == 0 ? 0.5 : -0.5;   // pre-collision state needs +F/2
+            u_out[3 * node] = (float)((jx + sh * S.P.F[0]) / rho);
+            u_out[3 * node + 1] = (float)((jy + sh * S.P.F[1]) / rho);
+            u_out[3 * node + 2] = (float)((jz + sh * S.P.F[2]) / rho);
+        }
+    }
+}
+
+// Host-side launchers, one per translation unit (FP64 is compiled without FMA
+// contraction to keep the reference's rounding).
+cudaError_t launch_step3d_f64(int npt, dim3 grid, cudaStream_t s, const StepArgs &a);
+cudaError_t launch_step3d_lp(int prec, int npt, dim3 grid, cudaStream_t s, const StepArgs &a);
+cudaError_t launch_init3d(int prec, void *A, long long plane, long long nn, cudaStream_t s);
+cudaError_t launch_canon3d(int prec, const Solve3 &S, long long done, double *f, float *u, cudaStream_t s);
+int max_blocks_step3d(int prec, int npt);
+
+}  // namespace lbm

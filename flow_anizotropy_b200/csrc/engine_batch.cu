@@ -1,0 +1,297 @@
+// liblbm batch engine: many resident 3D solves of one storage precision,
+// advanced together.  One persistent step kernel per time step walks a device
+// work list of (solve, tile) items covering every unfinished solve, each at
+// its own step count; a chunk of steps is one CUDA graph launch.  Solves
+// retire on the device (the controller marks them done) and are reclaimed by
+// lbm_batch_poll; new structures can be admitted between chunks, which is
+// what the serving loop uses for continuous batching.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm.h"
+#include "engine3d.cuh"
+#include "engine_host.h"
+
+using namespace lbm;
+
+namespace {
+
+struct Slot {
+    bool used = false;
+    bool retired = false;
+    long long tag = 0;
+    int dir = 0;
+    Solve3 S{};
+    std::shared_ptr<DevMem> mask;     // shared by the directions of one structure
+    DevMem lattice{nullptr};
+    DevMem partials{nullptr};
+    long long bytes = 0;
+};
+
+}  // namespace
+
+struct lbm_batch {
+    lbm_ctx *ctx = nullptr;
+    int precision = LBM_FP32;
+    int npt = 1;
+    int chunk = 64;
+    long long budget = 0;
+    long long resident = 0;
+    int cap_slots = 0;
+    int cap_work = 0;
+    int grid = 0;
+    std::vector<Slot> slots;
+    DevMem d_solves{nullptr}, d_states{nullptr}, d_work{nullptr}, d_nwork{nullptr};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<State3> hst;
+};
+
+static void destroy_graph(lbm_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+// One graph = `chunk` step launches (step index 0..chunk-1 relative to each
+// solve's s_base) followed by the s_base advance.
+static int capture(lbm_batch *b)
+{
+    lbm_ctx *ctx = b->ctx;
+    destroy_graph(b);
+    StepArgs a;
+    a.solves = static_cast<const Solve3 *>(b->d_solves.p);
+    a.work = static_cast<const int2 *>(b->d_work.p);
+    a.nwork_dev = static_cast<const int *>(b->d_nwork.p);
+    a.nwork = 0;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < b->chunk && e == cudaSuccess; ++i) {
+        a.step = i;
+        e = b->precision == LBM_FP64 ? launch_step3d_f64(b->npt, dim3(b->grid), ctx->stream, a)
+                                     : launch_step3d_lp(b->precision, b->npt, dim3(b->grid), ctx->stream, a);
+    }
+    if (e == cudaSuccess) {
+        advance3d_kernel<<<(b->cap_slots + 255) / 256, 256, 0, ctx->stream>>>(
+            static_cast<Solve3 *>(b->d_solves.p), b->cap_slots, b->chunk);
+        e = cudaGetLastError();
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);
+    if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return lbm_fail_cuda(ctx, e, "graph capture", __LINE__); }
+    CK(e2);
+    b->graph = g;
+    CK(cudaGraphInstantiate(&b->exec, g, 0));
+    return LBM_OK;
+}
+
+// Upload descriptors and the work list of every unfinished solve.
+static int sync_work(lbm_batch *b)
+{
+    lbm_ctx *ctx = b->ctx;
+    std::vector<Solve3> desc(b->cap_slots);
+    std::vector<int2> work;
+    for (int i = 0; i < b->cap_slots; ++i) {
+        const Slot &s = b->slots[i];
+        if (!s.used) {
+            // an empty slot: a descriptor whose state pointer marks it finished
+            desc[i] = Solve3{};
+            desc[i].st = static_cast<State3 *>(b->d_states.p) + i;
+            continue;
+        }
+        desc[i] = s.S;
+        if (!s.retired)
+            for (int t = 0; t < s.S.ntiles; ++t) work.push_back(make_int2(i, t));
+    }
+    if ((int)work.size() > b->cap_work) {
+        b->cap_work = std::max<int>((int)work.size(), 2 * b->cap_work);
+        CK(b->d_work.alloc(sizeof(int2) * (size_t)b->cap_work));
+        int rc = capture(b);
+        if (rc) return rc;
+    }
+    const int nwork = (int)work.size();
+    CK(cudaMemcpyAsync(b->d_solves.p, desc.data(), sizeof(Solve3) * b->cap_slots, cudaMemcpyHostToDevice, ctx->stream));
+    if (nwork)
+        CK(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, ctx->stream));
+    // pageable source: the copy is staged before the call returns
+    CK(cudaMemcpyAsync(b->d_nwork.p, &nwork, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return LBM_OK;
+}
+
+extern "C" long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int precision)
+{
+    const long long nn = (long long)nx * ny * nz;
+    const long long mask = 4ll * ((nx + 31) / 32) * (long long)ny * nz;
+    const long long tiles = (nn + TPB - 1) / TPB;
+    return mask + (long long)ndir * (lbm_lattice_bytes3d(nn, precision) + 24 * tiles);
+}
+
+extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, long long hbm_budget, int chunk)
+{
+    if (!ctx || !out) return LBM_EINPUT;
+    *out = nullptr;
+    CK(cudaSetDevice(ctx->device));
+    if (precision < LBM_FP64 || precision > LBM_BF16) return lbm_fail_input(ctx, "unknown precision");
+    if (chunk <= 0 || chunk > 4096) return lbm_fail_input(ctx, "chunk must be in 1..4096");
+    if (hbm_budget <= 0) return lbm_fail_input(ctx, "budget must be positive");
+    std::unique_ptr<lbm_batch> b(new lbm_batch());
+    b->ctx = ctx;
+    b->precision = precision;
+    b->chunk = chunk;
+    b->budget = hbm_budget;
+    b->npt = 1;
+    b->cap_slots = 4096;
+    b->cap_work = 1 << 16;
+    b->slots.resize(b->cap_slots);
+    b->hst.resize(b->cap_slots);
+    b->d_solves = DevMem(ctx->stream);
+    b->d_states = DevMem(ctx->stream);
+    b->d_work = DevMem(ctx->stream);
+    b->d_nwork = DevMem(ctx->stream);
+    for (auto &s : b->slots) { s.lattice = DevMem(ctx->stream); s.partials = DevMem(ctx->stream); }
+    CK(b->d_solves.alloc(sizeof(Solve3) * b->cap_slots));
+    CK(b->d_states.alloc(sizeof(State3) * b->cap_slots));
+    CK(b->d_work.alloc(sizeof(int2) * b->cap_work));
+    CK(b->d_nwork.alloc(sizeof(int)));
+    std::vector<State3> done(b->cap_slots);
+    for (auto &st : done) { memset(&st, 0, sizeof(st)); st.phase = PH_DONE; }
+    CK(cudaMemcpyAsync(b->d_states.p, done.data(), sizeof(State3) * b->cap_slots, cudaMemcpyHostToDevice, ctx->stream));
+    const int per_sm = std::max(1, max_blocks_step3d(precision, b->npt));
+    b->grid = ctx->sms * per_sm;
+    int rc = sync_work(b.get());
+    if (rc) return rc;
+    rc = capture(b.get());
+    if (rc) return rc;
+    *out = b.release();
+    return LBM_OK;
+}
+
+extern "C" void lbm_batch_destroy(lbm_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    destroy_graph(b);
+    delete b;
+}
+
+extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, int ny, int nz,
+                                  int ndir, const double *forces, const lbm_params3d *params, long long tag)
+{
+    if (!b) return LBM_EINPUT;
+    lbm_ctx *ctx = b->ctx;
+    if (!solid || !forces || !params || ndir <= 0) return lbm_fail_input(ctx, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    if (nx <= 0 || ny <= 0 || nz <= 0) return lbm_fail_input(ctx, "bad dimensions");
+    const long long nn = (long long)nx * ny * nz;
+    if (nn >= (1ll << 31) || (long long)Q3 * lbm_plane_elems(nn) >= (1ll << 32))
+        return lbm_fail_input(ctx, "lattice too large");
+    lbm_params3d p = *params;
+    if (p.precision != b->precision) return lbm_fail_input(ctx, "precision differs from the batch's");
+    p.npt = b->npt;
+    int rc = lbm_check_params3d(ctx, p);
+    if (rc) return rc;
+    const long long need = lbm_batch_bytes3d(nx, ny, nz, ndir, b->precision);
+    if (b->resident + need > b->budget) {
+        ctx->err = "batch budget exhausted";
+        return LBM_EBUSY;
+    }
+    std::vector<int> free_slots;
+    for (int i = 0; i < b->cap_slots && (int)free_slots.size() < ndir; ++i)
+        if (!b->slots[i].used) free_slots.push_back(i);
+    if ((int)free_slots.size() < ndir) { ctx->err = "batch slots exhausted"; return LBM_EBUSY; }
+
+    auto mask = std::make_shared<DevMem>(ctx->stream);
+    long long npore = 0;
+    rc = lbm_upload_mask(ctx, solid, nx, (long long)ny * nz, *mask, npore);
+    if (rc) return rc;
+    std::vector<State3> init(ndir);
+    for (int j = 0; j < ndir; ++j) {
+        Slot &s = b->slots[free_slots[j]];
+        lbm_fill_solve3(s.S, nx, ny, nz, forces + 3 * j, p, b->npt);
+        CK(s.lattice.alloc((size_t)lbm_lattice_bytes3d(nn, b->precision)));
+        CK(s.partials.alloc(sizeof(double) * 3 * (size_t)s.S.ntiles));
+        s.S.A = s.lattice.p;
+        s.S.mask = static_cast<const uint32_t *>(mask->p);
+        s.S.partials = static_cast<double *>(s.partials.p);
+        s.S.st = static_cast<State3 *>(b->d_states.p) + free_slots[j];
+        s.mask = mask;
+        s.tag = tag;
+        s.dir = j;
+        s.used = true;
+        s.retired = false;
+        s.bytes = lbm_lattice_bytes3d(nn, b->precision) + 24ll * s.S.ntiles;
+        lbm_init_state3(init[j], s.S.c);
+        CK(launch_init3d(b->precision, s.S.A, s.S.plane, s.S.nn, ctx->stream));
+        CK(cudaMemcpyAsync(s.S.st, &init[j], sizeof(State3), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    b->resident += need;
+    return sync_work(b);
+}
+
+extern "C" int lbm_batch_run(lbm_batch *b, int chunks)
+{
+    if (!b) return LBM_EINPUT;
+    lbm_ctx *ctx = b->ctx;
+    CK(cudaSetDevice(ctx->device));
+    for (int i = 0; i < chunks; ++i) CK(cudaGraphLaunch(b->exec, ctx->stream));
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_poll(lbm_batch *b, long long *tags, int *dirs, lbm_result3d *results, int max, int *n)
+{
+    if (!b || !n) return LBM_EINPUT;
+    lbm_ctx *ctx = b->ctx;
+    *n = 0;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(b->hst.data(), b->d_states.p, sizeof(State3) * b->cap_slots, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    bool changed = false;
+    for (int i = 0; i < b->cap_slots && *n < max; ++i) {
+        Slot &s = b->slots[i];
+        if (!s.used || s.retired) continue;
+        const State3 &st = b->hst[i];
+        if (st.phase < PH_DONE) continue;
+        lbm_result3d &r = results[*n];
+        for (int c = 0; c < 3; ++c) { r.q[c] = st.q[c]; r.se[c] = st.se[c]; }
+        r.steps = st.steps;
+        r.converged = st.converged;
+        r.status = st.status;
+        tags[*n] = s.tag;
+        dirs[*n] = s.dir;
+        ++*n;
+        s.retired = true;
+        s.used = false;
+        s.lattice.release();
+        s.partials.release();
+        b->resident -= s.bytes;
+        // the structure's mask goes with its last direction
+        const bool last = s.mask.use_count() == 1;
+        if (last) {
+            const long long nx = s.S.nx, ny = s.S.ny, nz = s.S.nz;
+            b->resident -= 4ll * ((nx + 31) / 32) * ny * nz;
+        }
+        s.mask.reset();
+        changed = true;
+    }
+    if (changed) return sync_work(b);
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_active(const lbm_batch *b)
+{
+    if (!b) return 0;
+    int n = 0;
+    for (const auto &s : b->slots) n += s.used && !s.retired;
+    return n;
+}
+
+extern "C" long long lbm_batch_resident_bytes(const lbm_batch *b) { return b ? b->resident : 0; }

@@ -1,0 +1,62 @@
+// Host-side pieces shared by the engine translation units (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+
+#include "../../include/lbm.h"
+#include "engine3d.cuh"
+
+struct lbm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sms = 0;
+    std::string err;
+};
+
+int lbm_fail_cuda(lbm_ctx *ctx, cudaError_t e, const char *what, int line);
+int lbm_fail_input(lbm_ctx *ctx, const std::string &msg);
+bool lbm_is_device_ptr(const void *p);
+std::string &lbm_last_error_global();
+
+#define CK(call)                                                              \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return lbm_fail_cuda(ctx, e_, #call, __LINE__); \
+    } while (0)
+
+// Stream-ordered device allocation released when the owner goes out of scope.
+struct DevMem {
+    void *p = nullptr;
+    cudaStream_t s = nullptr;
+    explicit DevMem(cudaStream_t st) : s(st) {}
+    DevMem(const DevMem &) = delete;
+    DevMem &operator=(const DevMem &) = delete;
+    DevMem(DevMem &&o) noexcept : p(o.p), s(o.s) { o.p = nullptr; }
+    DevMem &operator=(DevMem &&o) noexcept
+    {
+        if (this != &o) { release(); p = o.p; s = o.s; o.p = nullptr; }
+        return *this;
+    }
+    ~DevMem() { release(); }
+    cudaError_t alloc(size_t n)
+    {
+        release();
+        return cudaMallocAsync(&p, n ? n : 16, s);
+    }
+    void release()
+    {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+    }
+};
+
+int lbm_upload_mask(lbm_ctx *ctx, const uint8_t *solid, int nx, long long rows, DevMem &mask,
+                    long long &npore);
+int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p);
+long long lbm_plane_elems(long long nn);
+long long lbm_lattice_bytes3d(long long nn, int prec);
+void lbm_fill_solve3(lbm::Solve3 &S, int nx, int ny, int nz, const double F[3], const lbm_params3d &p, int npt);
+void lbm_init_state3(lbm::State3 &st, const lbm::Ctl3 &c);
+int lbm_pick_npt(const lbm_params3d &p);

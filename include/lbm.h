@@ -1,0 +1,189 @@
+/*
+ * liblbm — B200 lattice-Boltzmann permeability solver, C ABI.
+ *
+ * The reference has no library interface: its solvers are processes
+ * (LMB3d/lbm3d-perm.cpp:478-631, LMB2d/main.cpp:237-427) driven through
+ * subprocess by scripts/solve_permeability3d.py:113-146 and
+ * scripts/solve_permeability.py:29-46.  These entry points replace the
+ * in-process pieces of those binaries; the argv / CSV / exit-code surface is
+ * kept by the Python host (flow_anizotropy_b200.cli3d / cli2d), which calls
+ * this ABI through ctypes.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  `solid` and `vel_out` may be host or
+ *     device pointers (detected with cudaPointerGetAttributes); results are
+ *     host structs.
+ *   - Voxel order is x fastest, then y, then z (the .raw payload order,
+ *     scripts/structure_io3d.py:13-18); 1 = solid, 0 = pore.
+ *   - Return codes: LBM_OK (0) = all solves converged; LBM_NOT_CONVERGED (3)
+ *     = results valid but some `converged` flag is 0 (the reference's exit 3);
+ *     LBM_EINPUT (2) = bad input or non-finite flux (the reference's exit 2,
+ *     LMB3d/lbm3d-perm.cpp:140-144,339-341); LBM_EBUSY (4) = a batch has no
+ *     room; LBM_ECUDA (-1) = CUDA error.  Nothing here calls exit() or traps.
+ *     lbm_last_error() returns the message of the last failing call.
+ *   - One context per process and device; calls on one context are serialised
+ *     by the caller.  The library owns its lattice allocations.
+ */
+#ifndef LBM_H
+#define LBM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_API_VERSION 1
+
+#define LBM_OK             0
+#define LBM_EINPUT         2
+#define LBM_NOT_CONVERGED  3
+#define LBM_EBUSY          4
+#define LBM_ECUDA        (-1)
+
+/* Population storage (collision arithmetic is FP64 for LBM_FP64, else FP32;
+ * flux reductions, convergence test and averaging are FP64 in every mode). */
+#define LBM_FP64  0   /* f_k as double, the reference's own arithmetic           */
+#define LBM_FP32  1   /* shifted populations f_k - w_k as float                  */
+#define LBM_FP16  2   /* shifted populations, power-of-two scaled, IEEE half     */
+#define LBM_BF16  3   /* shifted populations as bfloat16                         */
+
+/* Phase-1 convergence criterion */
+#define LBM_CRIT_DRIFT  0  /* every lag steps: max_c |q_c - qprev_c| < eps ||q||
+                              (LMB3d/lbm3d-perm.cpp:332-360)                     */
+#define LBM_CRIT_BLOCK  1  /* block means over lag steps sampled every `sample`
+                              steps, accepted within max(eps ||m||, ksigma * SE)
+                              (the 2D reference's test, LMB2d/main.cpp:123-178) */
+
+typedef struct lbm_ctx lbm_ctx;
+
+/* Solver knobs of LMB3d/lbm3d-perm.cpp:118-130 plus tau (a compile-time
+ * constant there, :112), storage precision and criterion. */
+typedef struct {
+    double    tau;
+    double    eps;
+    long long lag;
+    long long min_steps;
+    long long max_steps;
+    long long avg_steps;
+    int       hold;
+    int       precision;
+    int       criterion;
+    int       npt;          /* nodes per thread of the step kernel (0 = auto) */
+    long long sample;       /* LBM_CRIT_BLOCK sample interval                 */
+    double    ksigma;       /* LBM_CRIT_BLOCK acceptance                      */
+} lbm_params3d;
+
+/* Per-direction result: struct Solve of LMB3d/lbm3d-perm.cpp:132-138. */
+typedef struct {
+    double    q[3];         /* Darcy flux mean(u) over ALL nodes              */
+    double    se[3];        /* standard error over the averaging phase        */
+    long long steps;
+    int       converged;
+    int       status;       /* LBM_OK or LBM_EINPUT (non-finite flux)         */
+} lbm_result3d;
+
+/* D2Q9 knobs of LMB2d/main.cpp:64-79 plus tau (LMB2d/lbm.cpp:86). */
+typedef struct {
+    double    tau;
+    double    eps;
+    long long lag;
+    long long min_steps;
+    long long max_steps;
+    long long avg_steps;
+    long long avg_sample;
+    double    qfloor;
+    double    ksigma;
+    int       hold;
+    int       reserved;
+} lbm_params2d;
+
+/* struct Solve of LMB2d/main.cpp:81-89 */
+typedef struct {
+    double    q[2];
+    double    se[2];
+    long long steps;
+    int       converged;
+    int       status;
+    double    fieldres;
+} lbm_result2d;
+
+/* ---- context ---------------------------------------------------------- */
+int         lbm_version(void);
+int         lbm_create(lbm_ctx **ctx, int device);
+void        lbm_destroy(lbm_ctx *ctx);
+const char *lbm_last_error(const lbm_ctx *ctx);
+
+/* ---- plain solves ----------------------------------------------------- */
+
+/* ndir forcing directions of one structure, each to convergence, concurrently
+ * (one lattice per direction, one launch per step for all of them).
+ * Replaces the three sequential solve() calls of LMB3d/lbm3d-perm.cpp:518-520
+ * (and the fourth, --validate, :558) together with read_structure (:174-193).
+ * forces: ndir x 3 doubles.  results: ndir.  vel_out: NULL or
+ * ndir x nx*ny*nz x 3 floats, the export_velocity field (:305-317) of each
+ * direction. */
+int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz,
+                int ndir, const double *forces, const lbm_params3d *params,
+                lbm_result3d *results, float *vel_out);
+
+/* D2Q9: solve() of LMB2d/main.cpp:99-235 with macro/collision/transport of
+ * LMB2d/lbm.cpp:563-632, for a runtime nx x ny cell (the reference is fixed
+ * at 256 x 256, LMB2d/lbm.h:24-25).  solid is ny x nx, x fastest.
+ * vel_out: NULL or ndir x nx*ny x 2 floats (U, V of the last step). */
+int lbm_solve2d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny,
+                int ndir, const double *forces, const lbm_params2d *params,
+                lbm_result2d *results, float *vel_out);
+
+/* ---- batched / served solves ------------------------------------------ */
+typedef struct lbm_batch lbm_batch;
+
+/* A resident set of 3D solves of one storage precision advanced together:
+ * each CUDA-graph launch runs `chunk` steps of every unfinished solve, each at
+ * its own step count; solves finish (retire) independently.  hbm_budget is
+ * the device memory the batch may hold for lattices, in bytes. */
+int  lbm_batch_create(lbm_ctx *ctx, lbm_batch **batch, int precision,
+                      long long hbm_budget, int chunk);
+void lbm_batch_destroy(lbm_batch *batch);
+
+/* Device bytes one structure with ndir directions occupies in a batch. */
+long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int precision);
+
+/* Admit one structure with ndir directions (results are reported per
+ * direction under (tag, dir)).  LBM_EBUSY if it does not fit the budget now. */
+int  lbm_batch_submit3d(lbm_batch *batch, const uint8_t *solid, int nx, int ny, int nz,
+                        int ndir, const double *forces, const lbm_params3d *params,
+                        long long tag);
+
+/* Advance every resident solve by `chunks` graph launches. */
+int  lbm_batch_run(lbm_batch *batch, int chunks);
+
+/* Retire finished solves: up to `max` (tag, dir, result) triples; *n gets
+ * the count.  Their memory returns to the budget. */
+int  lbm_batch_poll(lbm_batch *batch, long long *tags, int *dirs,
+                    lbm_result3d *results, int max, int *n);
+
+/* Unfinished solves in the batch, and the lattice bytes it holds now. */
+int       lbm_batch_active(const lbm_batch *batch);
+long long lbm_batch_resident_bytes(const lbm_batch *batch);
+
+/* ---- diagnostics (used by the parity tests) --------------------------- */
+
+/* Run exactly nsteps steps of one 3D solve and return the post-collision
+ * populations f*_k(x) in the reference's AoS order (N x 19 doubles; pores
+ * only, solids 0), the velocity of the last step (N x 3 floats) and the flux
+ * of the last step from the fused reduction.  Any output may be NULL. */
+int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz,
+                      const double force[3], double tau, int precision, int npt,
+                      long long nsteps, double *f_out, float *u_out, double q_out[3]);
+
+/* 2D counterpart: populations of the buffer the next step reads, ny x nx x 9
+ * floats, the U,V of the last step (ny x nx x 2) and its flux. */
+int lbm_debug_steps2d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny,
+                      const double force[2], double tau, long long nsteps,
+                      float *f_out, float *u_out, double q_out[2]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_H */
