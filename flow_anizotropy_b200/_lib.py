@@ -24,6 +24,7 @@ SYMBOLS = (
     "lbm_solve3d", "lbm_solve2d",
     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_bytes3d", "lbm_batch_submit3d",
     "lbm_batch_run", "lbm_batch_poll", "lbm_batch_active", "lbm_batch_resident_bytes",
+    "lbm_variant_count", "lbm_tune3d",
     "lbm_debug_steps3d", "lbm_debug_steps2d",
 )
 
@@ -32,7 +33,7 @@ class Params3D(C.Structure):
     _fields_ = [("tau", C.c_double), ("eps", C.c_double), ("lag", C.c_longlong),
                 ("min_steps", C.c_longlong), ("max_steps", C.c_longlong),
                 ("avg_steps", C.c_longlong), ("hold", C.c_int), ("precision", C.c_int),
-                ("criterion", C.c_int), ("npt", C.c_int), ("sample", C.c_longlong),
+                ("criterion", C.c_int), ("variant", C.c_int), ("sample", C.c_longlong),
                 ("ksigma", C.c_double)]
 
 
@@ -110,6 +111,11 @@ def load(path: Path | str | None = None):
         L.lbm_batch_active.restype = C.c_int
         L.lbm_batch_resident_bytes.argtypes = [vp]
         L.lbm_batch_resident_bytes.restype = C.c_longlong
+        L.lbm_variant_count.argtypes = [C.c_int]
+        L.lbm_variant_count.restype = C.c_int
+        L.lbm_tune3d.argtypes = [vp, u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                 dp, C.POINTER(C.c_int)]
+        L.lbm_tune3d.restype = C.c_int
         L.lbm_debug_steps3d.argtypes = [vp, u8p, C.c_int, C.c_int, C.c_int, dp, C.c_double,
                                         C.c_int, C.c_int, C.c_longlong, dp, fp, dp]
         L.lbm_debug_steps3d.restype = C.c_int

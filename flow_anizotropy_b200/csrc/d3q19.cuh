@@ -96,85 +96,122 @@ __device__ __forceinline__ void collide_ref64(double (&g)[Q3], const Phys3 &P,
 }
 
 // ---------------------------------------------------------------------------
-// FP32 operator on shifted populations h_k = f_k - w_k (rho0 = 1), the form
-// every reduced-precision storage uses.  Mathematically the same BGK + Guo
-// operator: rho = 1 + sum h, j = sum h e (sum w e = 0),
-//   h_eq = w (drho + rho (3 eu + 4.5 eu^2 - 1.5 u^2)),
-//   S_k  = w (1 - 1/2tau) [3 e.F - 3 u.F + 9 (e.u)(e.F)],
-//   h   <- h + (h_eq - h)/tau + S_k.
-// Keeping the O(u) deviations instead of O(1) populations removes the
-// cancellation that makes raw FP32 storage drift by ~1e-2 in k.
+// FP32 operator on shifted populations h_k = s (f_k - w_k) (rho0 = 1, s the
+// storage scale: a power of two for FP16, 1 otherwise), the form every
+// reduced-precision storage uses.  It is the same BGK + Guo operator:
+//   rho = 1 + sum h / s,  j = sum h e / s (sum w e = 0),
+//   h_eq = s w (drho + rho (3 eu + 4.5 eu^2 - 1.5 u^2)),
+//   S_k  = s w (1 - 1/2tau) [3 e.F - 3 u.F + 9 (e.u)(e.F)],
+//   h   <- h + (h_eq - h)/tau + S_k,
+// evaluated per opposite pair (k, opp k): e.u and e.F change sign, so each
+// pair shares one symmetric and one antisymmetric part and costs about half
+// of two separate directions.  Keeping the O(u) deviations instead of O(1)
+// populations removes the cancellation that makes raw FP32 storage drift by
+// ~1e-2 in k; working in scaled units leaves FP16 loads and stores a bare
+// conversion.  W1: tau == 1, where h drops out of the update.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void collide_shift32(float (&h)[Q3], const Phys3 &P,
-                                                float &ux, float &uy, float &uz)
+template <bool W1>
+__device__ __forceinline__ void collide_pairs(float (&h)[Q3], const Phys3 &P, float s, float is,
+                                              float &ux, float &uy, float &uz)
 {
-    float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+    // pair sums and differences; the odd member k of each pair is the "+" one
+    float sm[9], df[9];
 #pragma unroll
-    for (int k = 0; k < Q3; ++k) {
-        dr += h[k];
-        if (ex3(k) == 1) jx += h[k]; else if (ex3(k) == -1) jx -= h[k];
-        if (ey3(k) == 1) jy += h[k]; else if (ey3(k) == -1) jy -= h[k];
-        if (ez3(k) == 1) jz += h[k]; else if (ez3(k) == -1) jz -= h[k];
+    for (int p = 0; p < 9; ++p) {
+        sm[p] = h[2 * p + 1] + h[2 * p + 2];
+        df[p] = h[2 * p + 1] - h[2 * p + 2];
     }
+    float drs = h[0];
+#pragma unroll
+    for (int p = 0; p < 9; ++p) drs += sm[p];
+    float jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        const int k = 2 * p + 1;
+        if (ex3(k)) jx += ex3(k) > 0 ? df[p] : -df[p];
+        if (ey3(k)) jy += ey3(k) > 0 ? df[p] : -df[p];
+        if (ez3(k)) jz += ez3(k) > 0 ? df[p] : -df[p];
+    }
+    const float Fx = P.Ff[0], Fy = P.Ff[1], Fz = P.Ff[2];
+    const float dr = drs * is;
     const float rho = 1.0f + dr;
     const float ir = 1.0f / rho;
-    ux = (jx + 0.5f * P.Ff[0]) * ir;
-    uy = (jy + 0.5f * P.Ff[1]) * ir;
-    uz = (jz + 0.5f * P.Ff[2]) * ir;
+    ux = fmaf(jx, is, 0.5f * Fx) * ir;
+    uy = fmaf(jy, is, 0.5f * Fy) * ir;
+    uz = fmaf(jz, is, 0.5f * Fz) * ir;
     const float u2 = ux * ux + uy * uy + uz * uz;
-    const float uF = ux * P.Ff[0] + uy * P.Ff[1] + uz * P.Ff[2];
-    const float base = -1.5f * u2;
-    const float om = P.omega, pr = P.preff;
-    const float Fx = P.Ff[0], Fy = P.Ff[1], Fz = P.Ff[2];
+    const float uF = ux * Fx + uy * Fy + uz * Fz;
+    const float pr = P.preff;
+    const float srho = s * rho;
+    // per-node constants in scaled units
+    const float c1 = drs - 1.5f * srho * u2 - 3.0f * s * pr * uF;   // symmetric, eu = eF = 0 part
+    const float r45 = 4.5f * srho, r3 = 3.0f * srho;
+    const float p9 = 9.0f * s * pr, p3 = 3.0f * s * pr;
+    const float om = P.omega;
+    // rest population: h_eq + S = w0 c1
+    if constexpr (W1) h[0] = w3f(0) * c1;
+    else h[0] = fmaf(om, fmaf(w3f(0), c1 + 3.0f * s * pr * uF, -h[0]), h[0]) - w3f(0) * 3.0f * s * pr * uF;
 #pragma unroll
-    for (int k = 0; k < Q3; ++k) {
+    for (int p = 0; p < 9; ++p) {
+        const int k = 2 * p + 1;
         const int cx = ex3(k), cy = ey3(k), cz = ez3(k);
         float eu = 0.f, eF = 0.f;
         if (cx) { eu += cx > 0 ? ux : -ux; eF += cx > 0 ? Fx : -Fx; }
         if (cy) { eu += cy > 0 ? uy : -uy; eF += cy > 0 ? Fy : -Fy; }
         if (cz) { eu += cz > 0 ? uz : -uz; eF += cz > 0 ? Fz : -Fz; }
         const float w = w3f(k);
-        const float heq = w * (dr + rho * (eu * (3.0f + 4.5f * eu) + base));
-        const float sk = (w * pr) * (3.0f * eF * (1.0f + 3.0f * eu) - 3.0f * uF);
-        h[k] = h[k] + om * (heq - h[k]) + sk;
+        if constexpr (W1) {
+            // (h_eq + S)_k = sym + anti, (h_eq + S)_opp = sym - anti
+            const float sym = w * fmaf(fmaf(r45, eu, p9 * eF), eu, c1);
+            const float anti = w * fmaf(r3, eu, p3 * eF);
+            h[k] = sym + anti;
+            h[k + 1] = sym - anti;
+        } else {
+            // equilibrium and source split: E = Es +- Ea, S = Ss +- Sa
+            const float Es = w * fmaf(r45 * eu, eu, c1 + 3.0f * s * pr * uF);
+            const float Ea = w * r3 * eu;
+            const float Ss = w * fmaf(p9 * eF, eu, -3.0f * s * pr * uF);
+            const float Sa = w * p3 * eF;
+            h[k] = fmaf(om, (Es + Ea) - h[k], h[k]) + (Ss + Sa);
+            h[k + 1] = fmaf(om, (Es - Ea) - h[k + 1], h[k + 1]) + (Ss - Sa);
+        }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Storage formats.  Each exposes the element type, whether the stored value is
-// shifted (f - w), and load/store to the compute type.
+// Storage formats: element type, compute type, whether the stored value is
+// the (scaled) shifted population, and plain load/store conversions.
 // ---------------------------------------------------------------------------
 struct StoreF64 {
     using T = double; using C = double;
     static constexpr bool shifted = false;
     static constexpr int code = 0;
-    __device__ static __forceinline__ C ld(const T *p, float) { return *p; }
-    __device__ static __forceinline__ void st(T *p, C v, float) { *p = v; }
+    __device__ static __forceinline__ C ld(const T *p) { return *p; }
+    __device__ static __forceinline__ void st(T *p, C v) { *p = v; }
     __host__ __device__ static constexpr double init(int k) { return w3(k); }
 };
 struct StoreF32 {
     using T = float; using C = float;
     static constexpr bool shifted = true;
     static constexpr int code = 1;
-    __device__ static __forceinline__ C ld(const T *p, float) { return *p; }
-    __device__ static __forceinline__ void st(T *p, C v, float) { *p = v; }
+    __device__ static __forceinline__ C ld(const T *p) { return *p; }
+    __device__ static __forceinline__ void st(T *p, C v) { *p = v; }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 struct StoreF16 {
     using T = __half; using C = float;
     static constexpr bool shifted = true;
     static constexpr int code = 2;
-    // stored value = h * scale, scale a power of two chosen per solve
-    __device__ static __forceinline__ C ld(const T *p, float inv_scale) { return __half2float(*p) * inv_scale; }
-    __device__ static __forceinline__ void st(T *p, C v, float scale) { *p = __float2half_rn(v * scale); }
+    __device__ static __forceinline__ C ld(const T *p) { return __half2float(*p); }
+    __device__ static __forceinline__ void st(T *p, C v) { *p = __float2half_rn(v); }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 struct StoreBF16 {
     using T = __nv_bfloat16; using C = float;
     static constexpr bool shifted = true;
     static constexpr int code = 3;
-    __device__ static __forceinline__ C ld(const T *p, float) { return __bfloat162float(*p); }
-    __device__ static __forceinline__ void st(T *p, C v, float) { *p = __float2bfloat16_rn(v); }
+    __device__ static __forceinline__ C ld(const T *p) { return __bfloat162float(*p); }
+    __device__ static __forceinline__ void st(T *p, C v) { *p = __float2bfloat16_rn(v); }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 

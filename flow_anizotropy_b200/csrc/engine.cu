@@ -57,7 +57,8 @@ __global__ void pack_mask_kernel(const uint8_t *__restrict__ solid, int nx, long
         const uint8_t *row = solid + r * nx;
         uint32_t bits = 0;
         unsigned cnt = 0, b = 0;
-        for (int i = 0; i < 32 && x0 + i < nx; ++i) {
+        for (int i = 0; i < 32; ++i) {
+            if (x0 + i >= nx) { bits |= 1u << i; continue; }   // past the row end: solid
             const uint8_t v = row[x0 + i];
             b |= v > 1;
             if (v) bits |= 1u << i; else ++cnt;
@@ -148,8 +149,8 @@ int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
     if (p.criterion != LBM_CRIT_DRIFT && p.criterion != LBM_CRIT_BLOCK) return lbm_fail_input(ctx, "unknown criterion");
     if (p.criterion == LBM_CRIT_BLOCK && (p.sample <= 0 || p.lag % p.sample != 0))
         return lbm_fail_input(ctx, "block criterion needs sample > 0 dividing lag");
-    if (p.npt != 0 && p.npt != 1 && p.npt != 2 && !(p.npt == 4 && p.precision != LBM_FP64))
-        return lbm_fail_input(ctx, "npt must be 1, 2 or 4 (1 or 2 for FP64)");
+    if (p.variant < 0 || p.variant >= variant_count(p.precision))
+        return lbm_fail_input(ctx, "unknown step-kernel variant");
     return LBM_OK;
 }
 
@@ -210,15 +211,60 @@ void lbm_init_state3(State3 &st, const Ctl3 &c)
     }
 }
 
-int lbm_pick_npt(const lbm_params3d &p) { return p.npt > 0 ? p.npt : 1; }
+int lbm_pick_npt(const lbm_params3d &p) { return variant_npt(p.precision, p.variant); }
+
+int lbm_build_pores(lbm_ctx *ctx, Solve3 &S, int npt, DevMem &wpre, DevMem &fnode)
+{
+    const long long nwords = (long long)S.wpr * S.ny * S.nz;
+    const int blocks = (int)((nwords + SCAN_WORDS - 1) / SCAN_WORDS);
+    DevMem bsum(ctx->stream), boff(ctx->stream);
+    CK(bsum.alloc(sizeof(unsigned) * (size_t)blocks));
+    CK(boff.alloc(sizeof(unsigned) * (size_t)blocks));
+    CK(wpre.alloc(sizeof(uint32_t) * (size_t)(nwords + 1)));
+    word_sums_kernel<<<blocks, TPB, 0, ctx->stream>>>(S.mask, nwords, static_cast<unsigned *>(bsum.p));
+    CK(cudaGetLastError());
+    std::vector<unsigned> h(blocks);
+    CK(cudaMemcpyAsync(h.data(), bsum.p, sizeof(unsigned) * blocks, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long total = 0;
+    for (int b = 0; b < blocks; ++b) { const unsigned c = h[b]; h[b] = (unsigned)total; total += c; }
+    const uint32_t tot32 = (uint32_t)total;
+    CK(cudaMemcpyAsync(boff.p, h.data(), sizeof(unsigned) * blocks, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(static_cast<uint32_t *>(wpre.p) + nwords, &tot32, sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    word_scan_kernel<<<blocks, TPB, 0, ctx->stream>>>(S.mask, nwords, static_cast<const unsigned *>(boff.p),
+                                                      static_cast<uint32_t *>(wpre.p));
+    CK(cudaGetLastError());
+    CK(fnode.alloc(sizeof(uint32_t) * (size_t)std::max<unsigned long long>(total, 1)));
+    const int sb = (int)std::min<long long>((nwords + 255) / 256, 8L * 1184);
+    scatter_fnode_kernel<<<sb, 256, 0, ctx->stream>>>(S.mask, static_cast<const uint32_t *>(wpre.p), nwords,
+                                                      S.wpr, S.nx, static_cast<uint32_t *>(fnode.p));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));   // host staging must outlive the copies
+    S.wpre = static_cast<const uint32_t *>(wpre.p);
+    S.fnode = static_cast<const uint32_t *>(fnode.p);
+    S.nfluid = (int)total;
+    S.plane = lbm_plane_elems((long long)total);
+    S.ntiles = (int)((total + (unsigned long long)TPB * npt - 1) / ((unsigned long long)TPB * npt));
+    if (S.ntiles == 0) S.ntiles = 1;
+    return LBM_OK;
+}
+
+void lbm_copy_pores(Solve3 &dst, const Solve3 &src)
+{
+    dst.wpre = src.wpre; dst.fnode = src.fnode; dst.nfluid = src.nfluid;
+    dst.plane = src.plane; dst.ntiles = src.ntiles;
+}
 
 // Run a set of 3D solves sharing one mask to completion, one launch per step.
 // The host synchronises only where the controller can change phase: on lag
 // multiples and max_steps in phase 1, at the end of the averaging phase.
 static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, State3 *d_states,
-                       const int2 *d_work, int nwork, int prec, int npt, std::vector<State3> &hst)
+                       const int2 *d_work, int nwork, int prec, int variant, std::vector<State3> &hst)
 {
     const int n = (int)hs.size();
+    bool w1 = true;
+    for (const Solve3 &S : hs) w1 = w1 && S.P.tau == 1.0;
     long long s = 0;
     StepArgs a;
     a.solves = d_solves; a.work = d_work; a.nwork_dev = nullptr; a.nwork = nwork;
@@ -240,8 +286,8 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
         if (target == LLONG_MAX) break;
         for (; s < target; ++s) {
             a.step = s;
-            cudaError_t e = prec == LBM_FP64 ? launch_step3d_f64(npt, dim3(nwork), ctx->stream, a)
-                                             : launch_step3d_lp(prec, npt, dim3(nwork), ctx->stream, a);
+            cudaError_t e = prec == LBM_FP64 ? launch_step3d_f64(variant, dim3(nwork), ctx->stream, a)
+                                             : launch_step3d_lp(prec, variant, w1, dim3(nwork), ctx->stream, a);
             CK(e);
         }
     }
@@ -275,20 +321,27 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
     std::vector<DevMem> lat, part;
     lat.reserve(ndir); part.reserve(ndir);
     DevMem d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream);
+    DevMem wpre(ctx->stream), fnode(ctx->stream);
+    Solve3 proto;
+    lbm_fill_solve3(proto, nx, ny, nz, forces, p, npt);
+    proto.mask = static_cast<const uint32_t *>(mask.p);
+    rc = lbm_build_pores(ctx, proto, npt, wpre, fnode);
+    if (rc) return rc;
     CK(d_states.alloc(sizeof(State3) * ndir));
     for (int j = 0; j < ndir; ++j) {
         Solve3 &S = hs[j];
         lbm_fill_solve3(S, nx, ny, nz, forces + 3 * j, p, npt);
+        lbm_copy_pores(S, proto);
         lat.emplace_back(ctx->stream);
         part.emplace_back(ctx->stream);
-        CK(lat.back().alloc((size_t)lbm_lattice_bytes3d(nn, prec)));
+        CK(lat.back().alloc((size_t)lbm_lattice_bytes3d(S.nfluid, prec)));
         CK(part.back().alloc(sizeof(double) * 3 * (size_t)S.ntiles));
         S.A = lat.back().p;
         S.mask = static_cast<const uint32_t *>(mask.p);
         S.partials = static_cast<double *>(part.back().p);
         S.st = static_cast<State3 *>(d_states.p) + j;
         lbm_init_state3(hst[j], S.c);
-        CK(launch_init3d(prec, S.A, S.plane, S.nn, ctx->stream));
+        CK(launch_init3d(prec, S.A, S.plane, S.nfluid, ctx->stream));
     }
     std::vector<int2> work;
     for (int j = 0; j < ndir; ++j)
@@ -300,7 +353,7 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
     CK(cudaMemcpyAsync(d_states.p, hst.data(), sizeof(State3) * ndir, cudaMemcpyHostToDevice, ctx->stream));
 
     rc = run_plain3d(ctx, hs, static_cast<Solve3 *>(d_solves.p), static_cast<State3 *>(d_states.p),
-                     static_cast<const int2 *>(d_work.p), (int)work.size(), prec, npt, hst);
+                     static_cast<const int2 *>(d_work.p), (int)work.size(), prec, p.variant, hst);
     if (rc) return rc;
 
     if (vel_out) {
@@ -309,6 +362,7 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
         if (!dev) CK(vbuf.alloc(sizeof(float) * 3 * (size_t)nn));
         for (int j = 0; j < ndir; ++j) {
             float *dst = dev ? vel_out + 3 * nn * j : static_cast<float *>(vbuf.p);
+            CK(cudaMemsetAsync(dst, 0, sizeof(float) * 3 * (size_t)nn, ctx->stream));   // solids: u = 0
             CK(launch_canon3d(prec, hs[j], hst[j].steps, nullptr, dst, ctx->stream));
             if (!dev)
                 CK(cudaMemcpyAsync(vel_out + 3 * nn * j, vbuf.p, sizeof(float) * 3 * nn,
@@ -337,7 +391,7 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
 }
 
 extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz,
-                                 const double force[3], double tau, int precision, int npt,
+                                 const double force[3], double tau, int precision, int variant,
                                  long long nsteps, double *f_out, float *u_out, double q_out[3])
 {
     if (!ctx) return LBM_EINPUT;
@@ -350,10 +404,10 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     memset(&p, 0, sizeof(p));
     p.tau = tau; p.eps = 0.0; p.lag = LLONG_MAX / 4; p.hold = 1 << 30;
     p.min_steps = 0; p.max_steps = nsteps; p.avg_steps = 0;
-    p.precision = precision; p.criterion = LBM_CRIT_DRIFT; p.npt = npt; p.sample = 1;
+    p.precision = precision; p.criterion = LBM_CRIT_DRIFT; p.variant = variant; p.sample = 1;
     int rc = lbm_check_params3d(ctx, p);
     if (rc) return rc;
-    npt = lbm_pick_npt(p);
+    const int npt = lbm_pick_npt(p);
     DevMem mask(ctx->stream);
     long long npore = 0;
     rc = lbm_upload_mask(ctx, solid, nx, (long long)ny * nz, mask, npore);
@@ -363,13 +417,17 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     Solve3 &S = hs[0];
     lbm_fill_solve3(S, nx, ny, nz, force, p, npt);
     DevMem lat(ctx->stream), part(ctx->stream), d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream);
-    CK(lat.alloc((size_t)lbm_lattice_bytes3d(nn, precision)));
+    DevMem wpre(ctx->stream), fnode(ctx->stream);
+    S.mask = static_cast<const uint32_t *>(mask.p);
+    rc = lbm_build_pores(ctx, S, npt, wpre, fnode);
+    if (rc) return rc;
+    CK(lat.alloc((size_t)lbm_lattice_bytes3d(S.nfluid, precision)));
     CK(part.alloc(sizeof(double) * 3 * (size_t)S.ntiles));
     CK(d_states.alloc(sizeof(State3)));
     S.A = lat.p; S.mask = static_cast<const uint32_t *>(mask.p);
     S.partials = static_cast<double *>(part.p); S.st = static_cast<State3 *>(d_states.p);
     lbm_init_state3(hst[0], S.c);
-    CK(launch_init3d(precision, S.A, S.plane, S.nn, ctx->stream));
+    CK(launch_init3d(precision, S.A, S.plane, S.nfluid, ctx->stream));
     std::vector<int2> work;
     for (int t = 0; t < S.ntiles; ++t) work.push_back(make_int2(0, t));
     CK(d_solves.alloc(sizeof(Solve3)));
@@ -378,15 +436,123 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     CK(cudaMemcpyAsync(d_work.p, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(d_states.p, hst.data(), sizeof(State3), cudaMemcpyHostToDevice, ctx->stream));
     rc = run_plain3d(ctx, hs, static_cast<Solve3 *>(d_solves.p), static_cast<State3 *>(d_states.p),
-                     static_cast<const int2 *>(d_work.p), (int)work.size(), precision, npt, hst);
+                     static_cast<const int2 *>(d_work.p), (int)work.size(), precision, variant, hst);
     if (rc) return rc;
     DevMem fb(ctx->stream), ub(ctx->stream);
-    if (f_out) CK(fb.alloc(sizeof(double) * Q3 * (size_t)nn));
-    if (u_out) CK(ub.alloc(sizeof(float) * 3 * (size_t)nn));
+    if (f_out) {
+        CK(fb.alloc(sizeof(double) * Q3 * (size_t)nn));
+        CK(cudaMemsetAsync(fb.p, 0, sizeof(double) * Q3 * (size_t)nn, ctx->stream));
+    }
+    if (u_out) {
+        CK(ub.alloc(sizeof(float) * 3 * (size_t)nn));
+        CK(cudaMemsetAsync(ub.p, 0, sizeof(float) * 3 * (size_t)nn, ctx->stream));
+    }
     CK(launch_canon3d(precision, S, nsteps, static_cast<double *>(fb.p), static_cast<float *>(ub.p), ctx->stream));
     if (f_out) CK(cudaMemcpyAsync(f_out, fb.p, sizeof(double) * Q3 * nn, cudaMemcpyDeviceToHost, ctx->stream));
     if (u_out) CK(cudaMemcpyAsync(u_out, ub.p, sizeof(float) * 3 * nn, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (q_out) for (int c = 0; c < 3; ++c) q_out[c] = hst[0].q[c];
+    return LBM_OK;
+}
+
+extern "C" int lbm_variant_count(int precision)
+{
+    return (precision >= LBM_FP64 && precision <= LBM_BF16) ? variant_count(precision) : 0;
+}
+
+// Autotuner: every variant runs the same fixed number of steps on the same
+// resident lattices (directions as a batch, like a tensor solve), timed with
+// CUDA events on the launch stream.
+extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz, int ndir,
+                          int precision, int nsteps, double *ms_per_step, int *best)
+{
+    if (!ctx) return LBM_EINPUT;
+    CK(cudaSetDevice(ctx->device));
+    if (nx <= 0 || ny <= 0 || nz <= 0 || ndir <= 0 || nsteps <= 0) return lbm_fail_input(ctx, "bad arguments");
+    if (precision < LBM_FP64 || precision > LBM_BF16) return lbm_fail_input(ctx, "unknown precision");
+    const long long nn = (long long)nx * ny * nz;
+    if (nn >= (1ll << 31) || (long long)Q3 * lbm_plane_elems(nn) >= (1ll << 32))
+        return lbm_fail_input(ctx, "lattice too large");
+    DevMem mask(ctx->stream);
+    long long npore = 0;
+    int rc = lbm_upload_mask(ctx, solid, nx, (long long)ny * nz, mask, npore);
+    if (rc) return rc;
+    const int nv = variant_count(precision);
+    std::vector<DevMem> lat;
+    lat.reserve(ndir);
+    for (int j = 0; j < ndir; ++j) {
+        lat.emplace_back(ctx->stream);
+        CK(lat.back().alloc((size_t)lbm_lattice_bytes3d(npore, precision)));
+    }
+    DevMem d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream), part(ctx->stream);
+    CK(d_states.alloc(sizeof(State3) * ndir));
+    CK(d_solves.alloc(sizeof(Solve3) * ndir));
+    CK(part.alloc(sizeof(double) * 3 * (size_t)((nn + TPB - 1) / TPB + 1) * ndir));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double best_ms = 1e300;
+    int best_v = 0;
+    for (int v = 0; v < nv; ++v) {
+        lbm_params3d p;
+        memset(&p, 0, sizeof(p));
+        p.tau = 1.0; p.lag = LLONG_MAX / 4; p.hold = 1 << 30; p.max_steps = LLONG_MAX / 4;
+        p.precision = precision; p.variant = v; p.sample = 1;
+        const int npt = variant_npt(precision, v);
+        DevMem wpre(ctx->stream), fnode(ctx->stream);
+        Solve3 proto;
+        const double F0[3] = {1e-6, 0, 0};
+        lbm_fill_solve3(proto, nx, ny, nz, F0, p, npt);
+        proto.mask = static_cast<const uint32_t *>(mask.p);
+        rc = lbm_build_pores(ctx, proto, npt, wpre, fnode);
+        if (rc) break;
+        std::vector<Solve3> hs(ndir);
+        std::vector<State3> hst(ndir);
+        std::vector<int2> work;
+        for (int j = 0; j < ndir; ++j) {
+            double F[3] = {0, 0, 0};
+            F[j % 3] = 1e-6;
+            lbm_fill_solve3(hs[j], nx, ny, nz, F, p, npt);
+            lbm_copy_pores(hs[j], proto);
+            hs[j].A = lat[j].p;
+            hs[j].mask = proto.mask;
+            hs[j].partials = static_cast<double *>(part.p) + 3ll * j * ((nn + TPB - 1) / TPB + 1);
+            hs[j].st = static_cast<State3 *>(d_states.p) + j;
+            lbm_init_state3(hst[j], hs[j].c);
+            CK(launch_init3d(precision, hs[j].A, hs[j].plane, hs[j].nfluid, ctx->stream));
+            for (int t = 0; t < hs[j].ntiles; ++t) work.push_back(make_int2(j, t));
+        }
+        DevMem w(ctx->stream);
+        CK(w.alloc(sizeof(int2) * work.size()));
+        CK(cudaMemcpyAsync(w.p, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(d_solves.p, hs.data(), sizeof(Solve3) * ndir, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(d_states.p, hst.data(), sizeof(State3) * ndir, cudaMemcpyHostToDevice, ctx->stream));
+        StepArgs a;
+        a.solves = static_cast<const Solve3 *>(d_solves.p);
+        a.work = static_cast<const int2 *>(w.p);
+        a.nwork_dev = nullptr;
+        a.nwork = (int)work.size();
+        auto launch = [&](long long s) {
+            a.step = s;
+            return precision == LBM_FP64 ? launch_step3d_f64(v, dim3(a.nwork), ctx->stream, a)
+                                         : launch_step3d_lp(precision, v, true, dim3(a.nwork), ctx->stream, a);
+        };
+        long long s = 0;
+        for (int i = 0; i < std::max(2, nsteps / 4); ++i) CK(launch(s++));
+        CK(cudaEventRecord(e0, ctx->stream));
+        for (int i = 0; i < nsteps; ++i) CK(launch(s++));
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        const double per = (double)ms / nsteps;
+        if (ms_per_step) ms_per_step[v] = per;
+        if (per < best_ms) { best_ms = per; best_v = v; }
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (best) *best = best_v;
     return LBM_OK;
 }

@@ -3,23 +3,31 @@
 // controller that replaces the host loop of LMB3d/lbm3d-perm.cpp:320-398.
 //
 // Layout in HBM (one lattice per forcing direction):
-//   A[k][n]   19 planes, structure of arrays, n = (z*ny + y)*nx + x, plane
-//             stride padded to 128 B.  A single in-place buffer: the AA access
+//   A[k][i]   19 planes over the PORE voxels only, i = rank of the voxel among
+//             the pore voxels in x-fastest order (solids are never read by the
+//             reference, LMB3d/lbm3d-perm.cpp:261-265, so they get no storage);
+//             plane stride padded to 128 B.  One in-place buffer: the AA access
 //             pattern (Bailey et al. 2009) alternates
-//               odd steps  (local):     read A[k][n],        write A[opp k][n]
-//               even steps (neighbour): read A[opp k][n-e_k], write A[k][n+e_k]
+//               odd steps  (local):     read A[k][i],           write A[opp k][i]
+//               even steps (neighbour): read A[opp k][i(x-e_k)], write A[k][i(x+e_k)]
 //             so each location is read and then rewritten by the same thread
 //             and a step needs no second buffer.  Halfway bounce-back folds
 //             into the neighbour step: a link whose far end is solid reads
-//             A[k][n] and writes A[opp k][n] instead.  Step 1 of a solve is a
+//             A[k][i] and writes A[opp k][i] instead.  Step 1 of a solve is a
 //             local step on the initial state, which is exactly the reference's
 //             collide_only priming (LMB3d/lbm3d-perm.cpp:249-253,291-295).
-//   mask      1 bit per voxel, 1 = solid, rows of ceil(nx/32) words.
+//   mask      1 bit per voxel, 1 = solid, rows of ceil(nx/32) words (bits past
+//             nx in a row's last word set, i.e. solid).
+//   wpre      per mask word, the number of pore voxels before it (plus one
+//             final entry = pore count): the rank of voxel x in row r is
+//             wpre[r*wpr + x/32] + popc(~mask word & bits below x).
+//   fnode     linear index of each pore voxel (neighbour steps need x, y, z).
 //   partials  one double3 per tile, written only on reduction steps.
 //
-// Work is a list of (solve, tile) items; a tile is TPB*NPT consecutive nodes
-// of one lattice.  One launch advances every listed solve by one step, each at
-// its own step number, so solves admitted at different times share a launch.
+// Work is a list of (solve, tile) items; a tile is TPB*NPT consecutive pore
+// voxels of one lattice.  One launch advances every listed solve by one step,
+// each at its own step number, so solves admitted at different times share a
+// launch.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -86,11 +94,14 @@ struct State3 {
 
 struct Solve3 {
     void *A;
-    long long plane;      // elements per plane
+    long long plane;         // elements per plane (>= nfluid)
     const uint32_t *mask;
+    const uint32_t *wpre;    // pore voxels before each mask word (+ final total)
+    const uint32_t *fnode;   // pore voxels, ascending linear index
+    int nfluid;
     int nx, ny, nz, wpr;
     long long nn;
-    int ntiles;
+    int ntiles;              // tiles of TPB*NPT pore voxels
     FastDiv dvx, dvy;
     float scale, inv_scale;
     Phys3 P;
@@ -260,32 +271,14 @@ __device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long
     }
 }
 
-// Neighbourhood of one node: wrapped coordinates as offsets, so the linear
-// index of x + e_k is Zb[ez+1] + Yb[ey+1] + X[ex+1], and the solid bits of
-// the 18 neighbours (bit k set if x + e_k is solid; bit 0 = the node itself).
-struct Nbr3 {
-    int X[3];             // x-1, x, x+1 (wrapped)
-    int Yb[3];            // (y-1, y, y+1) * nx
-    int Zb[3];            // (z-1, z, z+1) * nx * ny
-    uint32_t solid;
-    __device__ __forceinline__ int idx(int k) const
-    {
-        return Zb[ez3(k) + 1] + Yb[ey3(k) + 1] + X[ex3(k) + 1];
-    }
+// Compact indices and solid bits of the 18 neighbours x + e_k of pore voxel
+// i at (x, y, z): bit k of `solid` is set if x + e_k is solid, idx[k] is the
+// pore rank of x + e_k (meaningful only when it is a pore).  Reads only the
+// mask and the word-prefix table, both small enough to stay in L1/L2.
+struct CNb {
+    unsigned idx[Q3];
+    unsigned solid;
 };
-
-// Bits of one mask row at x-1, x, x+1 (bit 0, 1, 2).  The word holding x
-// usually holds both neighbours; the two others are read only at word edges
-// and at the periodic wrap.
-__device__ __forceinline__ uint32_t row3(const uint32_t *__restrict__ row, int x, int xm, int xp)
-{
-    const uint32_t w = __ldg(row + (x >> 5));
-    const int b = x & 31;
-    const uint32_t c = (w >> b) & 1u;
-    const uint32_t m = (b != 0 && xm == x - 1) ? (w >> (b - 1)) & 1u : (uint32_t)mbit(row, xm);
-    const uint32_t p = (b != 31 && xp == x + 1) ? (w >> (b + 1)) & 1u : (uint32_t)mbit(row, xp);
-    return m | (c << 1) | (p << 2);
-}
 
 __host__ __device__ constexpr int k_of(int dx, int dy, int dz)
 {
@@ -294,46 +287,94 @@ __host__ __device__ constexpr int k_of(int dx, int dy, int dz)
     return -1;
 }
 
-__device__ __forceinline__ void neighbours3(const Solve3 &S, int x, int y, int z, Nbr3 &nb)
+__device__ __forceinline__ void compact_nbrs(const Solve3 &S, unsigned i, int x, int y, int z, CNb &nb)
 {
-    const int nx = S.nx, ny = S.ny, nz = S.nz;
-    const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+    const int nx = S.nx, ny = S.ny, nz = S.nz, wpr = S.wpr;
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
     const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
-    nb.X[0] = xm; nb.X[1] = x; nb.X[2] = xp;
-    nb.Yb[0] = ym * nx; nb.Yb[1] = y * nx; nb.Yb[2] = yp * nx;
-    const int zr[3] = {zm * ny, z * ny, zp * ny};
     const int yr[3] = {ym, y, yp};
-    nb.Zb[0] = zr[0] * nx; nb.Zb[1] = zr[1] * nx; nb.Zb[2] = zr[2] * nx;
-    uint32_t bits = 0;
+    const int zr[3] = {zm * ny, z * ny, zp * ny};
+    const int b = x & 31, wx = x >> 5;
+    const unsigned below = (1u << b) - 1u;
+    const bool xlo = x == 0, xhi = x == nx - 1;
+    const int xm = xlo ? nx - 1 : x - 1;
+    unsigned bits = 0;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
         for (int dy = -1; dy <= 1; ++dy) {
-            if (dy != 0 && dz != 0) {
-                // edge rows: only the x column is a D3Q19 neighbour
-                const uint32_t *row = S.mask + (size_t)(zr[dz + 1] + yr[dy + 1]) * S.wpr;
-                bits |= (uint32_t)mbit(row, x) << k_of(0, dy, dz);
-            } else {
-                const uint32_t *row = S.mask + (size_t)(zr[dz + 1] + yr[dy + 1]) * S.wpr;
-                const uint32_t b3 = row3(row, x, xm, xp);
-                bits |= ((b3 >> 1) & 1u) << k_of(0, dy, dz);
-                bits |= (b3 & 1u) << k_of(-1, dy, dz);
-                bits |= ((b3 >> 2) & 1u) << k_of(1, dy, dz);
+            const int row = zr[dz + 1] + yr[dy + 1];
+            const uint32_t *mrow = S.mask + (size_t)row * wpr;
+            const uint32_t *prow = S.wpre + (size_t)row * wpr;
+            const uint32_t m = __ldg(mrow + wx);
+            const unsigned s0 = (m >> b) & 1u;
+            const bool own = dy == 0 && dz == 0;
+            const unsigned A = own ? i : __ldg(prow + wx) + __popc(~m & below);
+            if (!own) {
+                nb.idx[k_of(0, dy, dz)] = A;
+                bits |= s0 << k_of(0, dy, dz);
+            }
+            if (dy == 0 || dz == 0) {
+                const int km = k_of(-1, dy, dz), kp = k_of(1, dy, dz);
+                unsigned sm, im, sp, ip;
+                if (!xlo) {
+                    sm = b ? (m >> (b - 1)) & 1u : __ldg(mrow + wx - 1) >> 31;
+                    im = A - 1u;
+                } else {               // periodic: x - 1 is the last voxel of the row
+                    sm = (__ldg(mrow + (xm >> 5)) >> (xm & 31)) & 1u;
+                    im = __ldg(prow + wpr) - 1u;
+                }
+                if (!xhi) {
+                    sp = b != 31 ? (m >> (b + 1)) & 1u : __ldg(mrow + wx + 1) & 1u;
+                    ip = A + 1u - s0;
+                } else {               // periodic: x + 1 is the first voxel of the row
+                    sp = __ldg(mrow) & 1u;
+                    ip = __ldg(prow);
+                }
+                nb.idx[km] = im;
+                nb.idx[kp] = ip;
+                bits |= (sm << km) | (sp << kp);
             }
         }
     nb.solid = bits;
 }
 
-// ----------------------------------------------------------- step kernel --
-// Resident blocks per SM the register allocation is sized for: enough
-// threads that roughly 40 KB of population loads are in flight per SM.
-template <class ST> struct MinBlocks { static constexpr int value = 2; };
-template <> struct MinBlocks<StoreF64> { static constexpr int value = 1; };
-template <> struct MinBlocks<StoreF32> { static constexpr int value = 2; };
+__device__ __forceinline__ void coords3(const Solve3 &S, unsigned node, int &x, int &y, int &z)
+{
+    const int r = S.dvx.div((int)node);
+    x = (int)node - r * S.nx;
+    z = S.dvy.div(r);
+    y = r - z * S.ny;
+}
 
-template <class ST, int NPT>
-__global__ void __launch_bounds__(TPB, MinBlocks<ST>::value) step3d_kernel(const StepArgs a)
+// Step-kernel variants: (pore voxels per thread, resident blocks per SM the
+// register allocation is sized for).  More resident blocks put more loads in
+// flight but force spills; lbm_tune3d times them on the actual structure.
+struct Variant { int npt, minb; };
+constexpr int NVAR_LP = 4, NVAR_F64 = 3;
+__host__ __device__ constexpr Variant variant_lp(int v)
+{
+    return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : v == 2 ? Variant{2, 3} : Variant{2, 2};
+}
+__host__ __device__ constexpr Variant variant_f64(int v)
+{
+    return v == 0 ? Variant{1, 2} : v == 1 ? Variant{1, 1} : Variant{2, 1};
+}
+
+// Collision dispatch: FP64 keeps the reference's arithmetic; reduced-precision
+// storage uses the pair-symmetric FP32 operator, specialised for tau = 1.
+template <class ST, bool W1, class Cp>
+__device__ __forceinline__ void collide3(Cp (&g)[Q3], const Solve3 &S, Cp &ux, Cp &uy, Cp &uz)
+{
+    if constexpr (ST::shifted) collide_pairs<W1>(g, S.P, S.scale, S.inv_scale, ux, uy, uz);
+    else collide_ref64(g, S.P, ux, uy, uz);
+}
+
+// One thread per pore voxel of a tile: every lane does useful work whatever
+// the porosity, and every access is to a pore voxel's own compact slot or to
+// a neighbour's.
+template <class ST, int NPT, int MINB, bool W1>
+__global__ void __launch_bounds__(TPB, MINB) step3d_kernel(const StepArgs a)
 {
     using T = typename ST::T;
     using Cp = typename ST::C;
@@ -349,67 +390,63 @@ __global__ void __launch_bounds__(TPB, MinBlocks<ST>::value) step3d_kernel(const
         const bool red = needs_reduction(S.c, phase, n);
         T *__restrict__ A = static_cast<T *>(S.A);
         const unsigned P = (unsigned)S.plane;        // 19 * plane < 2^32 (checked on the host)
-        const float sc = S.scale, isc = S.inv_scale;
         double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int j = 0; j < NPT; ++j) {
-            const long long node = (long long)item.y * (TPB * NPT) + j * TPB + threadIdx.x;
-            if (node >= S.nn) continue;
-            const int nd = (int)node;
-            const int r = S.dvx.div(nd);
-            const int x = nd - r * S.nx;
+            const unsigned i = (unsigned)(item.y * (TPB * NPT) + j * TPB + threadIdx.x);
+            if (i >= (unsigned)S.nfluid) continue;
+            Cp g[Q3];
+            Cp ux, uy, uz;
             if (!neighbour) {
-                if (mbit(S.mask + (size_t)r * S.wpr, x)) continue;
-                Cp g[Q3];
 #pragma unroll
-                for (int k = 0; k < Q3; ++k) g[k] = ST::ld(A + (k * P + (unsigned)nd), isc);
-                Cp ux, uy, uz;
-                if constexpr (ST::shifted) collide_shift32(g, S.P, ux, uy, uz);
-                else collide_ref64(g, S.P, ux, uy, uz);
+                for (int k = 0; k < Q3; ++k) g[k] = ST::ld(A + (k * P + i));
+                collide3<ST, W1>(g, S, ux, uy, uz);
 #pragma unroll
-                for (int k = 0; k < Q3; ++k) ST::st(A + (opp3(k) * P + (unsigned)nd), g[k], sc);
-                acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+                for (int k = 0; k < Q3; ++k) ST::st(A + (opp3(k) * P + i), g[k]);
             } else {
-                const int z = S.dvy.div(r);
-                const int y = r - z * S.ny;
-                Nbr3 nb;
-                neighbours3(S, x, y, z, nb);
-                if (nb.solid & 1u) continue;
-                Cp g[Q3];
-                g[0] = ST::ld(A + nd, isc);
+                int x, y, z;
+                coords3(S, __ldg(S.fnode + i), x, y, z);
+                CNb nb;
+                compact_nbrs(S, i, x, y, z, nb);
+                g[0] = ST::ld(A + i);
 #pragma unroll
                 for (int k = 1; k < Q3; ++k) {
-                    // pull from x - e_k = x + e_opp(k); bounce back if it is solid
+                    // pull from x - e_k = x + e_opp(k); bounce back if that is solid
                     const int o = opp3(k);
-                    g[k] = ((nb.solid >> o) & 1u) ? ST::ld(A + (k * P + (unsigned)nd), isc)
-                                                  : ST::ld(A + (o * P + (unsigned)nb.idx(o)), isc);
+                    const unsigned src = ((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]);
+                    g[k] = ST::ld(A + src);
                 }
-                Cp ux, uy, uz;
-                if constexpr (ST::shifted) collide_shift32(g, S.P, ux, uy, uz);
-                else collide_ref64(g, S.P, ux, uy, uz);
-                ST::st(A + nd, g[0], sc);
+                collide3<ST, W1>(g, S, ux, uy, uz);
+                ST::st(A + i, g[0]);
 #pragma unroll
                 for (int k = 1; k < Q3; ++k) {
-                    if ((nb.solid >> k) & 1u) ST::st(A + (opp3(k) * P + (unsigned)nd), g[k], sc);
-                    else ST::st(A + (k * P + (unsigned)nb.idx(k)), g[k], sc);
+                    const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
+                    ST::st(A + dst, g[k]);
                 }
-                acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
             }
+            acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
         if (red) finish_tile(S, item.y, n, acc, sh);
     }
 }
+
+// Pore-rank tables (once per structure).
+constexpr int SCAN_WORDS = 1024;    // mask words per block of the scan kernels
+__global__ void word_sums_kernel(const uint32_t *mask, long long nwords, unsigned *bsum);
+__global__ void word_scan_kernel(const uint32_t *mask, long long nwords, const unsigned *boff, uint32_t *wpre);
+__global__ void scatter_fnode_kernel(const uint32_t *mask, const uint32_t *wpre, long long nwords, int wpr,
+                                     int nx, uint32_t *fnode);
 
 // After a chunk of `steps` launches, solves still running have advanced by it.
 __global__ void advance3d_kernel(Solve3 *solves, int nsolves, long long steps);
 
 // Initial state: every population at rest (f = w, or h = 0 when shifted).
 template <class ST>
-__global__ void init3d_kernel(void *A, long long plane, long long nn)
+__global__ void init3d_kernel(void *A, long long plane, long long n)
 {
     using T = typename ST::T;
     T *a = static_cast<T *>(A);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
 #pragma unroll
         for (int k = 0; k < Q3; ++k) {
@@ -419,62 +456,60 @@ __global__ void init3d_kernel(void *A, long long plane, long long nn)
 }
 
 // Post-collision populations f*_k(x) of the last completed step `done`
-// (canonical, as the reference's f0 holds them), and/or the velocity of that
-// step recovered from them: Guo forcing gives j* = j + F, so
-// u = (j* - F/2) / rho.  Solid nodes get u = 0 and f = 0.
+// (canonical, as the reference's f0 holds them) into the dense AoS f_out, and/or
+// the velocity of that step recovered from them: Guo forcing gives
+// j* = j + F, so u = (j* - F/2) / rho.  Solid voxels are left untouched
+// (the caller zeroes the outputs).
 template <class ST>
 __global__ void canon3d_kernel(const Solve3 S, long long done, double *f_out, float *u_out)
 {
     using T = typename ST::T;
     const T *A = static_cast<const T *>(S.A);
-    const long long P = S.plane;
-    for (long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x; node < S.nn;
-         node += (long long)gridDim.x * blockDim.x) {
-        const int nd = (int)node;
-        const int r = S.dvx.div(nd);
-        const int x = nd - r * S.nx;
-        const int z = S.dvy.div(r);
-        const int y = r - z * S.ny;
-        Nbr3 nb;
-        neighbours3(S, x, y, z, nb);
-        if (nb.solid & 1u) {
-            if (f_out) for (int k = 0; k < Q3; ++k) f_out[node * Q3 + k] = 0.0;
-            if (u_out) { u_out[3 * node] = 0.f; u_out[3 * node + 1] = 0.f; u_out[3 * node + 2] = 0.f; }
-            continue;
-        }
+    const unsigned P = (unsigned)S.plane;
+    const double isc = (double)S.inv_scale;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < (unsigned)S.nfluid;
+         i += gridDim.x * blockDim.x) {
+        const unsigned node = S.fnode[i];
+        int x, y, z;
+        coords3(S, node, x, y, z);
+        CNb nb;
+        compact_nbrs(S, i, x, y, z, nb);
         double f[Q3];
 #pragma unroll
         for (int k = 0; k < Q3; ++k) {
             const int o = opp3(k);
-            double v;
-            if (done == 0) v = (double)ST::ld(A + k * P + nd, S.inv_scale);          // initial, pre-collision
-            else if (done & 1ll) v = (double)ST::ld(A + o * P + nd, S.inv_scale);     // after a local step
-            else if (k == 0) v = (double)ST::ld(A + nd, S.inv_scale);
-            else if ((nb.solid >> k) & 1u) v = (double)ST::ld(A + o * P + nd, S.inv_scale);
-            else v = (double)ST::ld(A + k * P + nb.idx(k), S.inv_scale);
-            f[k] = ST::shifted ? v + w3(k) : v;
+            unsigned at;
+            if (done == 0) at = k * P + i;                          // initial, pre-collision
+            else if (done & 1ll) at = o * P + i;                    // after a local step
+            else if (k == 0) at = i;
+            else if ((nb.solid >> k) & 1u) at = o * P + i;
+            else at = k * P + nb.idx[k];
+            const double v = (double)ST::ld(A + at);
+            f[k] = ST::shifted ? v * isc + w3(k) : v;
         }
         if (f_out)
-            for (int k = 0; k < Q3; ++k) f_out[node * Q3 + k] = f[k];
+            for (int k = 0; k < Q3; ++k) f_out[(size_t)node * Q3 + k] = f[k];
         if (u_out) {
             double rho = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
             for (int k = 0; k < Q3; ++k) {
                 rho += f[k]; jx += f[k] * ex3(k); jy += f[k] * ey3(k); jz += f[k] * ez3(k);
             }
             const double sh = done == 0 ? 0.5 : -0.5;   // pre-collision state needs +F/2
-            u_out[3 * node] = (float)((jx + sh * S.P.F[0]) / rho);
-            u_out[3 * node + 1] = (float)((jy + sh * S.P.F[1]) / rho);
-            u_out[3 * node + 2] = (float)((jz + sh * S.P.F[2]) / rho);
+            u_out[3 * (size_t)node] = (float)((jx + sh * S.P.F[0]) / rho);
+            u_out[3 * (size_t)node + 1] = (float)((jy + sh * S.P.F[1]) / rho);
+            u_out[3 * (size_t)node + 2] = (float)((jz + sh * S.P.F[2]) / rho);
         }
     }
 }
 
 // Host-side launchers, one per translation unit (FP64 is compiled without FMA
 // contraction to keep the reference's rounding).
-cudaError_t launch_step3d_f64(int npt, dim3 grid, cudaStream_t s, const StepArgs &a);
-cudaError_t launch_step3d_lp(int prec, int npt, dim3 grid, cudaStream_t s, const StepArgs &a);
-cudaError_t launch_init3d(int prec, void *A, long long plane, long long nn, cudaStream_t s);
+cudaError_t launch_step3d_f64(int variant, dim3 grid, cudaStream_t s, const StepArgs &a);
+cudaError_t launch_step3d_lp(int prec, int variant, bool w1, dim3 grid, cudaStream_t s, const StepArgs &a);
+cudaError_t launch_init3d(int prec, void *A, long long plane, long long n, cudaStream_t s);
 cudaError_t launch_canon3d(int prec, const Solve3 &S, long long done, double *f, float *u, cudaStream_t s);
-int max_blocks_step3d(int prec, int npt);
+int max_blocks_step3d(int prec, int variant);
+inline int variant_count(int prec) { return prec == 0 ? NVAR_F64 : NVAR_LP; }
+inline int variant_npt(int prec, int v) { return prec == 0 ? variant_f64(v).npt : variant_lp(v).npt; }
 
 }  // namespace lbm

@@ -28,9 +28,11 @@ struct Slot {
     int dir = 0;
     Solve3 S{};
     std::shared_ptr<DevMem> mask;     // shared by the directions of one structure
+    std::shared_ptr<DevMem> wpre, fnode;
     DevMem lattice{nullptr};
     DevMem partials{nullptr};
     long long bytes = 0;
+    long long tables = 0;     // mask + rank tables of the structure
 };
 
 }  // namespace
@@ -38,6 +40,8 @@ struct Slot {
 struct lbm_batch {
     lbm_ctx *ctx = nullptr;
     int precision = LBM_FP32;
+    int variant = 0;
+    bool w1 = true;
     int npt = 1;
     int chunk = 64;
     long long budget = 0;
@@ -75,8 +79,8 @@ static int capture(lbm_batch *b)
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < b->chunk && e == cudaSuccess; ++i) {
         a.step = i;
-        e = b->precision == LBM_FP64 ? launch_step3d_f64(b->npt, dim3(b->grid), ctx->stream, a)
-                                     : launch_step3d_lp(b->precision, b->npt, dim3(b->grid), ctx->stream, a);
+        e = b->precision == LBM_FP64 ? launch_step3d_f64(b->variant, dim3(b->grid), ctx->stream, a)
+                                     : launch_step3d_lp(b->precision, b->variant, b->w1, dim3(b->grid), ctx->stream, a);
     }
     if (e == cudaSuccess) {
         advance3d_kernel<<<(b->cap_slots + 255) / 256, 256, 0, ctx->stream>>>(
@@ -129,9 +133,10 @@ static int sync_work(lbm_batch *b)
 extern "C" long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int precision)
 {
     const long long nn = (long long)nx * ny * nz;
-    const long long mask = 4ll * ((nx + 31) / 32) * (long long)ny * nz;
+    // upper bound: every voxel a pore (the batch charges the exact size on admission)
+    const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 4ll * nn + 8;
     const long long tiles = (nn + TPB - 1) / TPB;
-    return mask + (long long)ndir * (lbm_lattice_bytes3d(nn, precision) + 24 * tiles);
+    return tables + (long long)ndir * (lbm_lattice_bytes3d(nn, precision) + 24 * tiles);
 }
 
 extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, long long hbm_budget, int chunk)
@@ -147,7 +152,8 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     b->precision = precision;
     b->chunk = chunk;
     b->budget = hbm_budget;
-    b->npt = 1;
+    b->variant = 0;
+    b->npt = variant_npt(precision, 0);
     b->cap_slots = 4096;
     b->cap_work = 1 << 16;
     b->slots.resize(b->cap_slots);
@@ -164,7 +170,7 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     std::vector<State3> done(b->cap_slots);
     for (auto &st : done) { memset(&st, 0, sizeof(st)); st.phase = PH_DONE; }
     CK(cudaMemcpyAsync(b->d_states.p, done.data(), sizeof(State3) * b->cap_slots, cudaMemcpyHostToDevice, ctx->stream));
-    const int per_sm = std::max(1, max_blocks_step3d(precision, b->npt));
+    const int per_sm = std::max(1, max_blocks_step3d(precision, b->variant));
     b->grid = ctx->sms * per_sm;
     int rc = sync_work(b.get());
     if (rc) return rc;
@@ -196,14 +202,9 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         return lbm_fail_input(ctx, "lattice too large");
     lbm_params3d p = *params;
     if (p.precision != b->precision) return lbm_fail_input(ctx, "precision differs from the batch's");
-    p.npt = b->npt;
+    p.variant = b->variant;
     int rc = lbm_check_params3d(ctx, p);
     if (rc) return rc;
-    const long long need = lbm_batch_bytes3d(nx, ny, nz, ndir, b->precision);
-    if (b->resident + need > b->budget) {
-        ctx->err = "batch budget exhausted";
-        return LBM_EBUSY;
-    }
     std::vector<int> free_slots;
     for (int i = 0; i < b->cap_slots && (int)free_slots.size() < ndir; ++i)
         if (!b->slots[i].used) free_slots.push_back(i);
@@ -213,11 +214,32 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
     long long npore = 0;
     rc = lbm_upload_mask(ctx, solid, nx, (long long)ny * nz, *mask, npore);
     if (rc) return rc;
+    auto wpre = std::make_shared<DevMem>(ctx->stream), fnode = std::make_shared<DevMem>(ctx->stream);
+    Solve3 proto;
+    lbm_fill_solve3(proto, nx, ny, nz, forces, p, b->npt);
+    proto.mask = static_cast<const uint32_t *>(mask->p);
+    rc = lbm_build_pores(ctx, proto, b->npt, *wpre, *fnode);
+    if (rc) return rc;
+    const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 4ll * proto.nfluid + 8;
+    const long long exact = tables + (long long)ndir * (lbm_lattice_bytes3d(proto.nfluid, b->precision) + 24ll * proto.ntiles);
+    if (b->resident + exact > b->budget) {
+        ctx->err = "batch budget exhausted";
+        return LBM_EBUSY;
+    }
+    if (p.tau != 1.0 && b->w1) {
+        // a relaxation time other than 1 needs the general collision kernel
+        b->w1 = false;
+        rc = capture(b);
+        if (rc) return rc;
+    }
     std::vector<State3> init(ndir);
     for (int j = 0; j < ndir; ++j) {
         Slot &s = b->slots[free_slots[j]];
         lbm_fill_solve3(s.S, nx, ny, nz, forces + 3 * j, p, b->npt);
-        CK(s.lattice.alloc((size_t)lbm_lattice_bytes3d(nn, b->precision)));
+        lbm_copy_pores(s.S, proto);
+        s.wpre = wpre; s.fnode = fnode;
+        s.tables = tables;
+        CK(s.lattice.alloc((size_t)lbm_lattice_bytes3d(s.S.nfluid, b->precision)));
         CK(s.partials.alloc(sizeof(double) * 3 * (size_t)s.S.ntiles));
         s.S.A = s.lattice.p;
         s.S.mask = static_cast<const uint32_t *>(mask->p);
@@ -228,12 +250,12 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         s.dir = j;
         s.used = true;
         s.retired = false;
-        s.bytes = lbm_lattice_bytes3d(nn, b->precision) + 24ll * s.S.ntiles;
+        s.bytes = lbm_lattice_bytes3d(s.S.nfluid, b->precision) + 24ll * s.S.ntiles;
         lbm_init_state3(init[j], s.S.c);
-        CK(launch_init3d(b->precision, s.S.A, s.S.plane, s.S.nn, ctx->stream));
+        CK(launch_init3d(b->precision, s.S.A, s.S.plane, s.S.nfluid, ctx->stream));
         CK(cudaMemcpyAsync(s.S.st, &init[j], sizeof(State3), cudaMemcpyHostToDevice, ctx->stream));
     }
-    b->resident += need;
+    b->resident += exact;
     return sync_work(b);
 }
 
@@ -275,11 +297,10 @@ extern "C" int lbm_batch_poll(lbm_batch *b, long long *tags, int *dirs, lbm_resu
         b->resident -= s.bytes;
         // the structure's mask goes with its last direction
         const bool last = s.mask.use_count() == 1;
-        if (last) {
-            const long long nx = s.S.nx, ny = s.S.ny, nz = s.S.nz;
-            b->resident -= 4ll * ((nx + 31) / 32) * ny * nz;
-        }
+        if (last) b->resident -= s.tables;
         s.mask.reset();
+        s.wpre.reset();
+        s.fnode.reset();
         changed = true;
     }
     if (changed) return sync_work(b);

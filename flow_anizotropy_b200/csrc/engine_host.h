@@ -60,3 +60,6 @@ long long lbm_lattice_bytes3d(long long nn, int prec);
 void lbm_fill_solve3(lbm::Solve3 &S, int nx, int ny, int nz, const double F[3], const lbm_params3d &p, int npt);
 void lbm_init_state3(lbm::State3 &st, const lbm::Ctl3 &c);
 int lbm_pick_npt(const lbm_params3d &p);
+// Pore-rank tables of a structure (wpre, fnode of S; nfluid, plane, ntiles for npt).
+int lbm_build_pores(lbm_ctx *ctx, lbm::Solve3 &S, int npt, DevMem &wpre, DevMem &fnode);
+void lbm_copy_pores(lbm::Solve3 &dst, const lbm::Solve3 &src);

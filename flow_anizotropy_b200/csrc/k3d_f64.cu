@@ -5,27 +5,31 @@
 
 namespace lbm {
 
-cudaError_t launch_step3d_f64(int npt, dim3 grid, cudaStream_t s, const StepArgs &a)
+#define LBM_F64(V) step3d_kernel<StoreF64, variant_f64(V).npt, variant_f64(V).minb, false>
+
+cudaError_t launch_step3d_f64(int variant, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
-    switch (npt) {
-    case 1: step3d_kernel<StoreF64, 1><<<grid, TPB, 0, s>>>(a); break;
-    case 2: step3d_kernel<StoreF64, 2><<<grid, TPB, 0, s>>>(a); break;
+    switch (variant) {
+    case 0: LBM_F64(0)<<<grid, TPB, 0, s>>>(a); break;
+    case 1: LBM_F64(1)<<<grid, TPB, 0, s>>>(a); break;
+    case 2: LBM_F64(2)<<<grid, TPB, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
-int max_blocks_f64(int npt)
+int max_blocks_f64(int variant)
 {
+    const void *k = variant == 0 ? (const void *)LBM_F64(0) : variant == 1 ? (const void *)LBM_F64(1)
+                                                                           : (const void *)LBM_F64(2);
     int nb = 0;
-    if (npt == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step3d_kernel<StoreF64, 1>, TPB, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step3d_kernel<StoreF64, 2>, TPB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;
 }
 
-cudaError_t launch_init3d_f64(void *A, long long plane, long long nn, cudaStream_t s)
+cudaError_t launch_init3d_f64(void *A, long long plane, long long n, cudaStream_t s)
 {
-    init3d_kernel<StoreF64><<<1184, 256, 0, s>>>(A, plane, nn);
+    init3d_kernel<StoreF64><<<1184, 256, 0, s>>>(A, plane, n);
     return cudaGetLastError();
 }
 

@@ -38,7 +38,7 @@ class Params3D:
     criterion: str = "auto"     # "drift" (reference), "block", or auto: block for fp16/bf16
     sample: int = 10
     ksigma: float = 3.0
-    npt: int = 0
+    variant: int = 0
 
     def to_c(self) -> _lib.Params3D:
         prec = _lib.PRECISIONS[self.precision]
@@ -49,7 +49,7 @@ class Params3D:
         return _lib.Params3D(tau=self.tau, eps=self.eps, lag=int(self.lag),
                              min_steps=int(self.min_steps), max_steps=int(self.max_steps),
                              avg_steps=int(self.avg_steps), hold=int(self.hold),
-                             precision=prec, criterion=crit_code, npt=int(self.npt),
+                             precision=prec, criterion=crit_code, variant=int(self.variant),
                              sample=int(self.sample), ksigma=float(self.ksigma))
 
 
@@ -158,7 +158,7 @@ def solve2d(solid, forces, params: Params2D | None = None, velocity: bool = Fals
     return out, rc, vel
 
 
-def debug_steps3d(solid, force, nsteps, tau=1.0, precision="fp64", npt=0, device=0):
+def debug_steps3d(solid, force, nsteps, tau=1.0, precision="fp64", variant=0, device=0):
     """Exactly ``nsteps`` steps; returns (f [z,y,x,19] float64, u [z,y,x,3] float32, q)."""
     ctx = _lib.context(device)
     arr = np.ascontiguousarray(solid, dtype=np.uint8)
@@ -168,7 +168,7 @@ def debug_steps3d(solid, force, nsteps, tau=1.0, precision="fp64", npt=0, device
     q = (C.c_double * 3)()
     Fv = (C.c_double * 3)(*[float(v) for v in force])
     rc = ctx.L.lbm_debug_steps3d(ctx.h, arr.ctypes.data_as(C.POINTER(C.c_uint8)), nx, ny, nz,
-                                 Fv, float(tau), _lib.PRECISIONS[precision], int(npt),
+                                 Fv, float(tau), _lib.PRECISIONS[precision], int(variant),
                                  int(nsteps), f.ctypes.data_as(C.POINTER(C.c_double)),
                                  u.ctypes.data_as(C.POINTER(C.c_float)), q)
     ctx.check(rc)
@@ -189,6 +189,20 @@ def debug_steps2d(solid, force, nsteps, tau=1.0, device=0):
                                  u.ctypes.data_as(C.POINTER(C.c_float)), q)
     ctx.check(rc)
     return f, u, np.array(q[:])
+
+
+def tune3d(solid, ndir=3, precision="fp32", nsteps=200, device=0):
+    """Time every step-kernel variant on this structure; returns (best, ms_per_step list)."""
+    ctx = _lib.context(device)
+    arr = np.ascontiguousarray(solid, dtype=np.uint8)
+    nz, ny, nx = arr.shape
+    prec = _lib.PRECISIONS[precision]
+    nv = ctx.L.lbm_variant_count(prec)
+    ms = (C.c_double * nv)()
+    best = C.c_int(0)
+    ctx.check(ctx.L.lbm_tune3d(ctx.h, arr.ctypes.data_as(C.POINTER(C.c_uint8)), nx, ny, nz,
+                               int(ndir), prec, int(nsteps), ms, C.byref(best)))
+    return int(best.value), list(ms)
 
 
 # --------------------------------------------------------------- batching ---
@@ -284,4 +298,4 @@ class Batch:
 
 
 __all__ = ["Params3D", "Result3D", "Params2D", "Result2D", "solve3d", "solve2d", "Batch",
-           "debug_steps3d", "debug_steps2d", "LBMError", "FX_BASE", "nu_of_tau"]
+           "debug_steps3d", "debug_steps2d", "tune3d", "LBMError", "FX_BASE", "nu_of_tau"]

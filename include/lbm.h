@@ -69,7 +69,7 @@ typedef struct {
     int       hold;
     int       precision;
     int       criterion;
-    int       npt;          /* nodes per thread of the step kernel (0 = auto) */
+    int       variant;      /* step-kernel variant (see lbm_tune3d); 0 = default */
     long long sample;       /* LBM_CRIT_BLOCK sample interval                 */
     double    ksigma;       /* LBM_CRIT_BLOCK acceptance                      */
 } lbm_params3d;
@@ -146,7 +146,9 @@ int  lbm_batch_create(lbm_ctx *ctx, lbm_batch **batch, int precision,
                       long long hbm_budget, int chunk);
 void lbm_batch_destroy(lbm_batch *batch);
 
-/* Device bytes one structure with ndir directions occupies in a batch. */
+/* Upper bound on the device bytes one structure with ndir directions
+ * occupies in a batch (as if every voxel were a pore; lattices hold pore
+ * voxels only, and admission charges the exact size). */
 long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int precision);
 
 /* Admit one structure with ndir directions (results are reported per
@@ -167,6 +169,19 @@ int  lbm_batch_poll(lbm_batch *batch, long long *tags, int *dirs,
 int       lbm_batch_active(const lbm_batch *batch);
 long long lbm_batch_resident_bytes(const lbm_batch *batch);
 
+/* ---- autotuning ------------------------------------------------------ */
+
+/* Number of step-kernel variants (pore voxels per thread x register budget)
+ * for a storage precision. */
+int lbm_variant_count(int precision);
+
+/* Time every step-kernel variant on this structure (ndir directions resident,
+ * `nsteps` timed steps each after a warm-up) with CUDA events; ms_per_step
+ * (may be NULL) receives lbm_variant_count(precision) values and *best the
+ * fastest variant.  No counterpart in the reference, which has one loop. */
+int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz, int ndir,
+               int precision, int nsteps, double *ms_per_step, int *best);
+
 /* ---- diagnostics (used by the parity tests) --------------------------- */
 
 /* Run exactly nsteps steps of one 3D solve and return the post-collision
@@ -174,7 +189,7 @@ long long lbm_batch_resident_bytes(const lbm_batch *batch);
  * only, solids 0), the velocity of the last step (N x 3 floats) and the flux
  * of the last step from the fused reduction.  Any output may be NULL. */
 int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz,
-                      const double force[3], double tau, int precision, int npt,
+                      const double force[3], double tau, int precision, int variant,
                       long long nsteps, double *f_out, float *u_out, double q_out[3]);
 
 /* 2D counterpart: populations of the buffer the next step reads, ny x nx x 9

@@ -70,3 +70,40 @@ def test_shifted_storage(gpu, prec, tol):
         scale = np.abs(fo[pore] - w).max()
         assert np.abs(d).max() <= tol * scale, (prec, n, np.abs(d).max() / scale)
         np.testing.assert_allclose(q, qo, rtol=tol * 5)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "fp16"])
+def test_every_variant_agrees(gpu, prec):
+    """Each step-kernel variant (pore voxels per thread x register budget) gives
+    the same populations: bit for bit within a precision."""
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200.solver import debug_steps3d
+    solid = _solid((10, 13, 37), 21)
+    force = [3e-7, 1e-6, 0]
+    nv = _lib.load().lbm_variant_count(_lib.PRECISIONS[prec])
+    ref = None
+    for v in range(nv):
+        for n in (3, 4):
+            f, u, q = debug_steps3d(solid, force, n, precision=prec, variant=v)
+            if v == 0:
+                ref = (ref or {})
+                ref[n] = (f, q)
+            else:
+                assert np.array_equal(f, ref[n][0]), (prec, v, n)
+                np.testing.assert_allclose(q, ref[n][1], rtol=1e-12)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp32", 2e-6), ("fp16", 2e-3)])
+def test_shifted_storage_general_tau(gpu, prec, tol):
+    """tau != 1 takes the general (non-specialised) pair operator."""
+    from flow_anizotropy_b200.solver import debug_steps3d
+    solid = _solid((12, 14, 16), 9)
+    force = [0, 0, 1e-6]
+    w = np.array([1/3] + [1/18] * 6 + [1/36] * 12)
+    for n in (1, 2, 5):
+        f, u, q = debug_steps3d(solid, force, n, tau=0.8, precision=prec)
+        fo, uo, qo = _oracle_after(solid, force, n, tau=0.8)
+        pore = solid == 0
+        d = (f[pore] - w) - (fo[pore] - w)
+        scale = np.abs(fo[pore] - w).max()
+        assert np.abs(d).max() <= tol * scale, (prec, n, np.abs(d).max() / scale)
