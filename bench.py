@@ -1,0 +1,402 @@
+#!/usr/bin/env python3
+"""Benchmark: k-tensors/hour and GLUPS of the B200 permeability solver.
+
+Workload (one bench step = one full permeability tensor): the 128^3 packing
+of overlapping prolate ellipsoids, semi-axes (4, 4, 12) voxels along z,
+porosity 0.45, percolating in x, y and z (seeded, synthetic), solved along
++x, +y and +z with g = 1e-6 (--ff 4), tau = 1, eps = 1e-6 relative drift every
+1000 steps, hold 2, min 4000, max 50000 steps, 2000 averaging steps.  The
+three directions run concurrently on one GPU.
+
+Reported (one JSON line, rank 0):
+  value      k-tensors/hour of the headline path (default: FP16 shifted
+             storage, FP32 collision, FP64 reductions), inputs resident in HBM,
+             device time from CUDA events on the solver's stream;
+  e2e        the same through the public API with the structure in host memory
+             (host->device copy and result read-back inside the timed region);
+  plain_fp32 the same workload with plain FP32 storage, one launch per step;
+  rel_err    the headline K against the FP64 K of the same structure;
+  roofline   HBM roofline of the step kernel: algorithmic bytes (pore voxels
+             x 2 x 19 x element size + N/8 mask) / time, against the measured
+             copy bandwidth;
+  cpu_baseline  the reference CPU solver (oracle/_ref/lbm3d-perm, built from
+             the reference sources) on all host cores, a bounded fixed-step
+             sample, extrapolated to a converged tensor with the FP64 step
+             counts.
+
+Multi-GPU (torchrun): every rank solves its own tensors, no collective in the
+data path ("weak" scaling); the timed region is bracketed by a barrier and the
+max over ranks is reported.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp16]
+    python bench.py --impl reference        # the reference CPU solver alone
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "k-tensors/hr & GLUPS at ≤1e-3 rel err vs FP64, vs plain FP32; p50/p99 latency"
+WORKLOAD = dict(workload="perm-tensor 128^3 prolate-ellipsoid packing (4,4,12) phi=0.45, 3 directions",
+                n=128, semi=(4.0, 4.0, 12.0), porosity=0.45, seed=0, ff=4.0, tau=1.0, eps=1e-6,
+                lag=1000, hold=2, min_steps=4000, max_steps=50000, avg_steps=2000)
+BYTES_PER_UPDATE = {"fp64": 304, "fp32": 152, "fp16": 76, "bf16": 76}
+# Steps per direction of the converged FP64 solve of the workload structure
+# (x, y, z).  Our FP64 path reproduces the reference's step counts exactly
+# (per-step bit-identical populations; see tests/test_gpu_solve3d.py); the
+# reference arm uses these to turn its fixed-step sample into a full tensor.
+FP64_STEPS = (8000, 7000, 8000)
+
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------- clocks --
+class Clocks:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.f = tempfile.TemporaryFile(mode="w+")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.device)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.f:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ----------------------------------------------------------------- helpers --
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per step launch of the headline kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "step3d_tensor128.md"
+    if p.exists():
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def tensor_K(runs, mu, F):
+    return np.array([[mu * runs[j].q[c] / F for j in range(3)] for c in range(3)])
+
+
+def k_errors(K, K64):
+    """Per-entry relative error of K against the FP64 K; off-diagonals are
+    judged against the trace scale (they are ~0 for this axis-aligned packing)."""
+    scale = np.abs(np.diag(K64)).max()
+    diag = float(max(abs(K[i, i] - K64[i, i]) / abs(K64[i, i]) for i in range(3)))
+    off = float(max(abs(K[i, j] - K64[i, j]) for i in range(3) for j in range(3) if i != j) / scale)
+    return {"max_rel_diag": diag, "max_offdiag_over_kmax": off, "max_rel": max(diag, off)}
+
+
+class EventTimer:
+    """CUDA events on the solver's stream (every kernel of the context runs there)."""
+
+    def __init__(self, torch, stream_ptr):
+        self.torch = torch
+        self.stream = torch.cuda.ExternalStream(stream_ptr)
+
+    def __enter__(self):
+        self.e0 = self.torch.cuda.Event(enable_timing=True)
+        self.e1 = self.torch.cuda.Event(enable_timing=True)
+        self.torch.cuda.synchronize()
+        self.e0.record(self.stream)
+        return self
+
+    def __exit__(self, *exc):
+        self.e1.record(self.stream)
+        self.e1.synchronize()
+        self.torch.cuda.synchronize()
+        self.ms = self.e0.elapsed_time(self.e1)
+
+
+# ------------------------------------------------------------ CPU baseline --
+def cpu_sample(solid, wl, seconds_target=12.0, steps=None):
+    """Reference binary (or the oracle port) on all host cores, fixed-step sample.
+
+    Returns dict(lups_per_core, cores, kind, sample, seconds)."""
+    from oracle import oracle as O
+    from flow_anizotropy_b200.structure_io3d import save_structure
+    cores = os.cpu_count() or 1
+    nz, ny, nx = solid.shape
+    N = solid.size
+    ref = O.ref_binary("lbm3d-perm")
+    if steps is None:
+        steps = max(2, int(seconds_target * 12e6 / (3 * N)))       # ~12 MLUPS per core
+    tmp = Path(tempfile.mkdtemp(prefix="lbmcpu_"))
+    raw = tmp / "s.raw"
+    save_structure(raw, solid)
+    t0 = time.perf_counter()
+    if ref is not None:
+        kind = "reference"
+        args = ["--quiet", "--ff", str(wl["ff"]), "--max-steps", str(steps), "--min-steps", str(steps + 1),
+                "--lag", str(steps + 1), "--avg-steps", "0"]
+        procs = [subprocess.Popen([str(ref), str(raw), str(tmp / f"o{i}.csv")] + args,
+                                  stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for i in range(cores)]
+        for p in procs:
+            p.wait()
+        dirs = 3
+    else:
+        kind = "port"
+        cores = 1
+        st = O.State3D(solid, wl["tau"])
+        st.reset([2.5e-7 * wl["ff"], 0, 0])
+        st.step(steps)
+        dirs = 1
+    dt = time.perf_counter() - t0
+    shutil.rmtree(tmp, ignore_errors=True)
+    lups = dirs * steps * N / dt          # all-node convention, per process
+    return dict(lups_per_core=lups, cores=cores, kind=kind, seconds=dt,
+                sample=f"{dirs} x {steps} fixed steps of the {nx}x{ny}x{nz} workload structure per process, "
+                       f"{cores} processes")
+
+
+def cpu_baseline_entry(cpu, N, steps64):
+    """k-tensors/hour of the CPU solver extrapolated with the FP64 step counts."""
+    lu_tensor = N * float(sum(steps64))
+    sec_tensor = lu_tensor / cpu["lups_per_core"]
+    return {"value": 3600.0 * cpu["cores"] / sec_tensor, "unit": "k-tensors/hr", "cores": cpu["cores"],
+            "kind": cpu["kind"], "sample": cpu["sample"] + "; extrapolated with FP64 step counts "
+            f"{list(map(int, steps64))}", "mlups_per_core": cpu["lups_per_core"] / 1e6}
+
+
+# -------------------------------------------------------------- our arm ----
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200 import solver as S
+    from flow_anizotropy_b200 import structures as st
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    device = local_rank
+    torch.cuda.set_device(device)
+    wl = dict(WORKLOAD)
+    solid = st.ellipsoid_packing(wl["n"], wl["semi"], wl["porosity"], wl["seed"])
+    N = solid.size
+    npore = int((solid == 0).sum())
+    F = 2.5e-7 * wl["ff"]
+    forces = [[F, 0, 0], [0, F, 0], [0, 0, F]]
+    mu = (1.0 / 3.0) * (wl["tau"] - 0.5)
+    ctx = _lib.context(device)
+    solid_dev = torch.from_numpy(np.ascontiguousarray(solid)).cuda(device)
+
+    def params(prec, variant=0):
+        return S.Params3D(tau=wl["tau"], eps=wl["eps"], lag=wl["lag"], hold=wl["hold"], min_steps=wl["min_steps"],
+                          max_steps=wl["max_steps"], avg_steps=wl["avg_steps"], precision=prec,
+                          criterion="auto", variant=variant)
+
+    # FP64 oracle solve on the GPU (the reference's arithmetic), untimed
+    r64, _, _ = S.solve3d(solid_dev, forces, params("fp64"), device=device)
+    K64 = tensor_K(r64, mu, F)
+    steps64 = [r.steps for r in r64]
+
+    def measure(prec, warmup, steps, host_input=False):
+        best, ms = S.tune3d(solid, ndir=3, precision=prec, nsteps=100, device=device)
+        p = params(prec, best)
+        inp = solid if host_input else solid_dev
+        for _ in range(warmup):
+            S.solve3d(inp, forces, p, device=device)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        runs_all = []
+        with Clocks(device) as clk, EventTimer(torch, ctx.stream) as t:
+            for _ in range(steps):
+                runs, rc, _ = S.solve3d(inp, forces, p, device=device)
+                runs_all.append(runs)
+        torch.cuda.synchronize()
+        ms_total = t.ms
+        if dist is not None:
+            tt = torch.tensor([ms_total], dtype=torch.float64, device=f"cuda:{device}")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms_total = float(tt.item())
+        dir_steps = sum(sum(r.steps for r in runs) for runs in runs_all)
+        launches = sum(max(r.steps for r in runs) for runs in runs_all)
+        return dict(prec=prec, variant=best, tune_ms=ms, ms=ms_total, runs=runs_all[-1], clocks=clk.summary(),
+                    dir_steps=dir_steps, launches=launches)
+
+    head = measure(args.precision, args.warmup, args.steps)
+    plain = measure("fp32", max(1, min(args.warmup, 2)), max(1, min(args.steps, 3)))
+    e2e = measure(args.precision, 1, args.steps, host_input=True)
+
+    def rates(m):
+        sec = m["ms"] / 1e3
+        tensors = world * (args.steps if m is not plain else max(1, min(args.steps, 3)))
+        kt_hr = 3600.0 * tensors / sec
+        glups_fluid = world * m["dir_steps"] * npore / sec / 1e9
+        glups_all = world * m["dir_steps"] * N / sec / 1e9
+        return kt_hr, glups_fluid, glups_all
+
+    kt, gf, ga = rates(head)
+    kt_p, gf_p, ga_p = rates(plain)
+    kt_e, _, _ = rates(e2e)
+    Kh = tensor_K(head["runs"], mu, F)
+    Kp = tensor_K(plain["runs"], mu, F)
+    peak, peak_kind = measured_peak()
+    B = BYTES_PER_UPDATE[args.precision]
+    alg_bytes = head["dir_steps"] * (npore * B + N / 8.0)
+    achieved = alg_bytes / (head["ms"] / 1e3) / 1e9
+    per_launch_alg = alg_bytes / max(1, head["launches"])
+    traffic = profiled_traffic()
+    out = None
+    if rank == 0:
+        cpu = cpu_sample(solid, wl, seconds_target=args.cpu_seconds)
+        cpu_entry = cpu_baseline_entry(cpu, N, steps64)
+        out = {
+            "metric": METRIC, "value": kt, "unit": "k-tensors/hr", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": {"fp16": "f16-storage/f32-compute/f64-reduce",
+                                                              "bf16": "bf16-storage/f32-compute/f64-reduce",
+                                                              "fp32": "f32", "fp64": "f64"}[args.precision],
+            "data": "synthetic (seeded structure; no dataset)",
+            "config": {"workload": wl["workload"], "seed": wl["seed"], "tau": wl["tau"], "g": F,
+                       "eps": wl["eps"], "lag": wl["lag"], "max_steps": wl["max_steps"],
+                       "precision": args.precision, "kernel_variant": head["variant"],
+                       "criterion": "block-mean k-sigma" if args.precision in ("fp16", "bf16") else "drift (reference)",
+                       "parallelism": f"work partition x{world} (one tensor stream per GPU)",
+                       "l2": "lattice (3 x 19 x pores x elem) exceeds L2 only for fp32/fp64; each tensor is a "
+                             "fresh solve streaming its lattice every step"},
+            "glups_fluid": gf, "glups_all_node": ga,
+            "steps_per_direction": [r.steps for r in head["runs"]],
+            "converged": [r.converged for r in head["runs"]],
+            "rel_err_vs_fp64": k_errors(Kh, K64),
+            "plain_fp32": {"value": kt_p, "unit": "k-tensors/hr", "glups_fluid": gf_p, "glups_all_node": ga_p,
+                           "steps_per_direction": [r.steps for r in plain["runs"]],
+                           "rel_err_vs_fp64": k_errors(Kp, K64), "kernel_variant": plain["variant"]},
+            "speedup_vs_plain_fp32": kt / kt_p,
+            "fp64_steps_per_direction": steps64,
+            "e2e": {"value": kt_e, "unit": "k-tensors/hr", "h2d_bytes_per_step": int(N),
+                    "d2h_bytes_per_step": int(3 * 64)},
+            "gpu_launches": int(head["launches"] + 8 * args.steps),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "alg_bytes_per_launch": per_launch_alg,
+                         "kernel": f"step3d_kernel<{args.precision}, variant {head['variant']}>"},
+            "cpu_baseline": cpu_entry,
+            "clocks": head["clocks"],
+        }
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+# -------------------------------------------------------- reference arm ----
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from flow_anizotropy_b200 import structures as st
+    wl = dict(WORKLOAD)
+    solid = st.ellipsoid_packing(wl["n"], wl["semi"], wl["porosity"], wl["seed"])
+    N = solid.size
+    steps64 = FP64_STEPS
+    per_step = []
+    cpu = None
+    for i in range(args.warmup + args.steps):
+        cpu = cpu_sample(solid, wl, seconds_target=args.cpu_seconds)
+        if i >= args.warmup:
+            per_step.append(cpu)
+    lups = statistics.median(c["lups_per_core"] for c in per_step)
+    cpu = dict(per_step[-1], lups_per_core=lups)
+    entry = cpu_baseline_entry(cpu, N, steps64)
+    return {"metric": METRIC, "value": entry["value"], "unit": "k-tensors/hr", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * float(sum(steps64)) * N / (lups * cpu["cores"]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded structure)",
+            "config": {"workload": wl["workload"], "seed": wl["seed"], "precision": "fp64"},
+            "impl": "reference", "cpu_baseline": entry,
+            "e2e": {"value": entry["value"], "unit": "k-tensors/hr", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16", "fp32", "fp64"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_ours(args, rank, world, local_rank)
+    if out is not None and rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -20,7 +20,7 @@ CRIT_DRIFT, CRIT_BLOCK = 0, 1
 
 # Exported symbols, exactly those include/lbm.h declares.
 SYMBOLS = (
-    "lbm_version", "lbm_create", "lbm_destroy", "lbm_last_error",
+    "lbm_version", "lbm_create", "lbm_destroy", "lbm_last_error", "lbm_stream",
     "lbm_solve3d", "lbm_solve2d",
     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_bytes3d", "lbm_batch_submit3d",
     "lbm_batch_run", "lbm_batch_poll", "lbm_batch_active", "lbm_batch_resident_bytes",
@@ -87,6 +87,8 @@ def load(path: Path | str | None = None):
         L.lbm_destroy.restype = None
         L.lbm_last_error.argtypes = [vp]
         L.lbm_last_error.restype = C.c_char_p
+        L.lbm_stream.argtypes = [vp]
+        L.lbm_stream.restype = C.c_void_p
         L.lbm_solve3d.argtypes = [vp, u8p, C.c_int, C.c_int, C.c_int, C.c_int, dp,
                                   C.POINTER(Params3D), C.POINTER(Result3D), fp]
         L.lbm_solve3d.restype = C.c_int
@@ -137,6 +139,11 @@ class Context:
             raise LBMError(rc, "lbm_create failed: " + self.L.lbm_last_error(None).decode())
         self.h = h
         self.device = device
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the context, as an integer (for torch.cuda.ExternalStream)."""
+        return int(self.L.lbm_stream(self.h) or 0)
 
     def error(self) -> str:
         return self.L.lbm_last_error(self.h).decode()

@@ -135,6 +135,8 @@ std::string &lbm_last_error_global()
     return s;
 }
 
+extern "C" void *lbm_stream(const lbm_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
 extern "C" const char *lbm_last_error(const lbm_ctx *ctx)
 {
     return ctx ? ctx->err.c_str() : lbm_last_error_global().c_str();

@@ -113,6 +113,9 @@ int         lbm_version(void);
 int         lbm_create(lbm_ctx **ctx, int device);
 void        lbm_destroy(lbm_ctx *ctx);
 const char *lbm_last_error(const lbm_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), on which every kernel of the
+ * context is launched: for timing with CUDA events from the caller. */
+void       *lbm_stream(const lbm_ctx *ctx);
 
 /* ---- plain solves ----------------------------------------------------- */
 
