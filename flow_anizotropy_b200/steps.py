@@ -1,0 +1,44 @@
+"""Run a fixed number of solver steps on a named workload (for profiling).
+
+    python -m flow_anizotropy_b200.steps --workload tensor128 --precision fp16 --steps 24
+
+Builds the seeded structure, solves the three forcing directions together for
+exactly --steps steps (no convergence stop, no averaging) and prints the
+fluxes.  `ncu -k regex:step3d -s S -c C` on this command captures step
+launches of the same kernels the benchmark runs.
+"""
+from __future__ import annotations
+
+import argparse
+
+from . import solver as S
+from . import structures as st
+
+WORKLOADS = {
+    "tensor128": lambda: st.precision_128(0),
+    "plain64": lambda: st.plain_64(0),
+}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--workload", default="tensor128", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "fp16", "bf16"])
+    ap.add_argument("--variant", type=int, default=-1, help="step-kernel variant (-1: autotune)")
+    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--tau", type=float, default=1.0)
+    a = ap.parse_args(argv)
+    solid = WORKLOADS[a.workload]()
+    variant = a.variant
+    if variant < 0:
+        variant, _ = S.tune3d(solid, ndir=3, precision=a.precision, nsteps=50)
+    F = 1e-6
+    p = S.Params3D(precision=a.precision, criterion="drift", tau=a.tau, lag=10**9, max_steps=a.steps,
+                   avg_steps=0, hold=10**6, variant=variant)
+    runs, rc, _ = S.solve3d(solid, [[F, 0, 0], [0, F, 0], [0, 0, F]], p)
+    for r in runs:
+        print(r.steps, r.q)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,96 @@
+"""Batched solves (lbm_batch_*): many structures of uneven size resident
+together, advanced by CUDA-graph chunks, retiring independently.  Every
+result must equal the same solve run alone (the flux reduction sums tiles in
+a fixed order, so alone and in the mix agree bit for bit), and admission must
+respect the HBM budget."""
+import numpy as np
+import pytest
+
+from flow_anizotropy_b200 import solver as S
+from flow_anizotropy_b200 import structures as st
+
+pytestmark = pytest.mark.gpu
+
+PRM = dict(eps=1e-6, lag=100, hold=2, min_steps=200, max_steps=3000, avg_steps=50)
+
+
+def _mix():
+    out = []
+    for i, (shape, r, phi) in enumerate([((16, 18, 20), 3.0, 0.6), ((24, 24, 24), 4.0, 0.5),
+                                         ((12, 20, 33), 3.0, 0.55), ((20, 16, 16), 3.5, 0.65)]):
+        out.append(st.sphere_packing(shape, r, phi, seed=40 + i, percolate=(True, True, True)))
+    return out
+
+
+def _forces(F=1e-6):
+    return [[F, 0, 0], [0, F, 0], [0, 0, F]]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16"])
+def test_batch_equals_alone(gpu, prec):
+    structs = _mix()
+    p = S.Params3D(precision=prec, **PRM)
+    b = S.Batch(precision=prec, hbm_budget=4 * 2**30, chunk=32)
+    for t, s in enumerate(structs):
+        assert b.submit(s, _forces(), p, tag=t)
+    done = {}
+    for _ in range(1000):
+        b.run(4)
+        for tag, runs in b.poll():
+            done[tag] = runs
+        if len(done) == len(structs):
+            break
+    assert len(done) == len(structs) and b.active() == 0
+    assert b.resident_bytes() == 0
+    for t, s in enumerate(structs):
+        alone, rc, _ = S.solve3d(s, _forces(), p)
+        for a, m in zip(alone, done[t]):
+            assert a.steps == m.steps and a.converged == m.converged
+            assert np.array_equal(a.q, m.q), (prec, t, a.q, m.q)
+            assert np.array_equal(a.se, m.se)
+
+
+def test_batch_admission_and_continuous(gpu):
+    """A budget that holds two structures: the third is refused until one
+    retires, then admitted while the others keep running."""
+    structs = _mix()[:3]
+    p = S.Params3D(precision="fp32", **PRM)
+    need = max(S.Batch.bytes_needed(s.shape, 3, "fp32") for s in structs)
+    b = S.Batch(precision="fp32", hbm_budget=int(2.2 * need), chunk=16)
+    assert b.submit(structs[0], _forces(), p, tag=0)
+    assert b.submit(structs[1], _forces(), p, tag=1)
+    admitted_late = b.submit(structs[2], _forces(), p, tag=2)
+    done = {}
+    for _ in range(2000):
+        b.run(2)
+        for tag, runs in b.poll():
+            done[tag] = runs
+        if not admitted_late:
+            admitted_late = b.submit(structs[2], _forces(), p, tag=2)
+        if len(done) == 3:
+            break
+    assert len(done) == 3
+    alone, _, _ = S.solve3d(structs[2], _forces(), p)
+    for a, m in zip(alone, done[2]):
+        assert a.steps == m.steps and np.array_equal(a.q, m.q)
+
+
+def test_batch_mixed_tau(gpu):
+    """A solve with tau != 1 switches the batch to the general collision."""
+    s = _mix()[0]
+    p1 = S.Params3D(precision="fp32", **PRM)
+    p8 = S.Params3D(precision="fp32", tau=0.8, **PRM)
+    b = S.Batch(precision="fp32", hbm_budget=2**30, chunk=16)
+    assert b.submit(s, _forces(), p1, tag=0)
+    assert b.submit(s, _forces(), p8, tag=1)
+    done = {}
+    for _ in range(2000):
+        b.run(4)
+        done.update(dict(b.poll()))
+        if len(done) == 2:
+            break
+    for tag, p in ((0, p1), (1, p8)):
+        alone, _, _ = S.solve3d(s, _forces(), p)
+        for a, m in zip(alone, done[tag]):
+            assert a.steps == m.steps
+            np.testing.assert_allclose(m.q, a.q, rtol=1e-6, atol=1e-20)
