@@ -28,6 +28,7 @@ UNITS = {
     "k3d_f64.cu": ["-fmad=false"],
     "k2d.cu": ["-fmad=false"],
     "k3d_lp.cu": [],
+    "k3d_m.cu": [],
     "engine.cu": [],
     "engine2.cu": [],
     "engine_batch.cu": [],

@@ -14,6 +14,7 @@
 #include "../../include/lbm.h"
 #include "engine2d.cuh"
 #include "engine_host.h"
+#include "engine_m.cuh"
 
 using namespace lbm;
 
@@ -147,7 +148,9 @@ int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
 {
     if (!(p.tau > 0.5)) return lbm_fail_input(ctx, "tau must exceed 0.5");
     if (p.lag <= 0) return lbm_fail_input(ctx, "--lag must be positive");
-    if (p.precision < LBM_FP64 || p.precision > LBM_BF16) return lbm_fail_input(ctx, "unknown precision");
+    if (p.precision < LBM_FP64 || p.precision > LBM_M64) return lbm_fail_input(ctx, "unknown precision");
+    if (is_moment(p.precision) && p.tau != 1.0)
+        return lbm_fail_input(ctx, "moment-projected storage needs tau = 1");
     if (p.criterion != LBM_CRIT_DRIFT && p.criterion != LBM_CRIT_BLOCK) return lbm_fail_input(ctx, "unknown criterion");
     if (p.criterion == LBM_CRIT_BLOCK && (p.sample <= 0 || p.lag % p.sample != 0))
         return lbm_fail_input(ctx, "block criterion needs sample > 0 dividing lag");
@@ -160,14 +163,47 @@ static size_t elem_size(int prec) { return prec == LBM_FP64 ? 8 : (prec == LBM_F
 
 long long lbm_plane_elems(long long nn) { return (nn + 63) / 64 * 64; }
 
-long long lbm_lattice_bytes3d(long long nn, int prec)
+// Lattice bytes of one direction over n pore voxels.
+long long lbm_lattice_bytes3d(long long n, int prec)
 {
-    return (long long)Q3 * lbm_plane_elems(nn) * (long long)elem_size(prec);
+    if (is_moment(prec)) return 2ll * 16ll * mom_buffer_elems(prec, n);
+    return (long long)Q3 * lbm_plane_elems(n) * (long long)elem_size(prec);
+}
+
+// Plane stride (populations) or buffer length in 16-byte elements (moments).
+long long lbm_plane_for(int prec, long long n)
+{
+    return is_moment(prec) ? mom_buffer_elems(prec, n) : lbm_plane_elems(n);
+}
+
+cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
+{
+    if (prec == LBM_FP64) return launch_step3d_f64(variant, odd, grid, s, a);
+    if (is_moment(prec)) return launch_stepm(prec, variant, grid, s, a);
+    return launch_step3d_lp(prec, variant, w1, odd, grid, s, a);
+}
+
+int lbm_max_blocks(int prec, int variant, bool odd)
+{
+    return is_moment(prec) ? max_blocks_stepm(prec, variant) : max_blocks_step3d(prec, variant, odd);
+}
+
+cudaError_t lbm_init_lattice(int prec, const Solve3 &S, cudaStream_t s)
+{
+    if (is_moment(prec)) return cudaSuccess;        // step 1 writes the moments from scratch
+    return launch_init3d(prec, S.A, S.plane, S.nfluid, s);
+}
+
+cudaError_t lbm_canon(int prec, const Solve3 &S, long long done, double *f, float *u, cudaStream_t s)
+{
+    if (is_moment(prec)) return launch_canonm(prec, S, done, f, u, s);
+    return launch_canon3d(prec, S, done, f, u, s);
 }
 
 void lbm_fill_solve3(Solve3 &S, int nx, int ny, int nz, const double F[3], const lbm_params3d &p, int npt)
 {
     memset(&S, 0, sizeof(S));
+    S.prec = p.precision;
     S.nx = nx; S.ny = ny; S.nz = nz;
     S.wpr = (nx + 31) / 32;
     S.nn = (long long)nx * ny * nz;
@@ -246,7 +282,7 @@ int lbm_build_pores(lbm_ctx *ctx, Solve3 &S, int npt, DevMem &wpre, DevMem &fnod
     S.wpre = static_cast<const uint32_t *>(wpre.p);
     S.fnode = static_cast<const uint32_t *>(fnode.p);
     S.nfluid = (int)total;
-    S.plane = lbm_plane_elems((long long)total);
+    S.plane = lbm_plane_for(S.prec, (long long)total);
     S.ntiles = (int)((total + (unsigned long long)TPB * npt - 1) / ((unsigned long long)TPB * npt));
     if (S.ntiles == 0) S.ntiles = 1;
     return LBM_OK;
@@ -288,9 +324,8 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
         if (target == LLONG_MAX) break;
         for (; s < target; ++s) {
             a.step = s;
-            cudaError_t e = prec == LBM_FP64 ? launch_step3d_f64(variant, dim3(nwork), ctx->stream, a)
-                                             : launch_step3d_lp(prec, variant, w1, dim3(nwork), ctx->stream, a);
-            CK(e);
+            // every solve of the call is at step s + 1 (they start together)
+            CK(lbm_launch_step(prec, variant, w1, ((s + 1) & 1) == 1, dim3(nwork), ctx->stream, a));
         }
     }
     return LBM_OK;
@@ -343,7 +378,7 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
         S.partials = static_cast<double *>(part.back().p);
         S.st = static_cast<State3 *>(d_states.p) + j;
         lbm_init_state3(hst[j], S.c);
-        CK(launch_init3d(prec, S.A, S.plane, S.nfluid, ctx->stream));
+        CK(lbm_init_lattice(prec, S, ctx->stream));
     }
     std::vector<int2> work;
     for (int j = 0; j < ndir; ++j)
@@ -365,7 +400,7 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
         for (int j = 0; j < ndir; ++j) {
             float *dst = dev ? vel_out + 3 * nn * j : static_cast<float *>(vbuf.p);
             CK(cudaMemsetAsync(dst, 0, sizeof(float) * 3 * (size_t)nn, ctx->stream));   // solids: u = 0
-            CK(launch_canon3d(prec, hs[j], hst[j].steps, nullptr, dst, ctx->stream));
+            CK(lbm_canon(prec, hs[j], hst[j].steps, nullptr, dst, ctx->stream));
             if (!dev)
                 CK(cudaMemcpyAsync(vel_out + 3 * nn * j, vbuf.p, sizeof(float) * 3 * nn,
                                    cudaMemcpyDeviceToHost, ctx->stream));
@@ -429,7 +464,7 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     S.A = lat.p; S.mask = static_cast<const uint32_t *>(mask.p);
     S.partials = static_cast<double *>(part.p); S.st = static_cast<State3 *>(d_states.p);
     lbm_init_state3(hst[0], S.c);
-    CK(launch_init3d(precision, S.A, S.plane, S.nfluid, ctx->stream));
+    CK(lbm_init_lattice(precision, S, ctx->stream));
     std::vector<int2> work;
     for (int t = 0; t < S.ntiles; ++t) work.push_back(make_int2(0, t));
     CK(d_solves.alloc(sizeof(Solve3)));
@@ -449,7 +484,7 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
         CK(ub.alloc(sizeof(float) * 3 * (size_t)nn));
         CK(cudaMemsetAsync(ub.p, 0, sizeof(float) * 3 * (size_t)nn, ctx->stream));
     }
-    CK(launch_canon3d(precision, S, nsteps, static_cast<double *>(fb.p), static_cast<float *>(ub.p), ctx->stream));
+    CK(lbm_canon(precision, S, nsteps, static_cast<double *>(fb.p), static_cast<float *>(ub.p), ctx->stream));
     if (f_out) CK(cudaMemcpyAsync(f_out, fb.p, sizeof(double) * Q3 * nn, cudaMemcpyDeviceToHost, ctx->stream));
     if (u_out) CK(cudaMemcpyAsync(u_out, ub.p, sizeof(float) * 3 * nn, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -459,7 +494,7 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
 
 extern "C" int lbm_variant_count(int precision)
 {
-    return (precision >= LBM_FP64 && precision <= LBM_BF16) ? variant_count(precision) : 0;
+    return (precision >= LBM_FP64 && precision <= LBM_M64) ? variant_count(precision) : 0;
 }
 
 // Autotuner: every variant runs the same fixed number of steps on the same
@@ -471,7 +506,7 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
     if (!ctx) return LBM_EINPUT;
     CK(cudaSetDevice(ctx->device));
     if (nx <= 0 || ny <= 0 || nz <= 0 || ndir <= 0 || nsteps <= 0) return lbm_fail_input(ctx, "bad arguments");
-    if (precision < LBM_FP64 || precision > LBM_BF16) return lbm_fail_input(ctx, "unknown precision");
+    if (precision < LBM_FP64 || precision > LBM_M64) return lbm_fail_input(ctx, "unknown precision");
     const long long nn = (long long)nx * ny * nz;
     if (nn >= (1ll << 31) || (long long)Q3 * lbm_plane_elems(nn) >= (1ll << 32))
         return lbm_fail_input(ctx, "lattice too large");
@@ -521,7 +556,7 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
             hs[j].partials = static_cast<double *>(part.p) + 3ll * j * ((nn + TPB - 1) / TPB + 1);
             hs[j].st = static_cast<State3 *>(d_states.p) + j;
             lbm_init_state3(hst[j], hs[j].c);
-            CK(launch_init3d(precision, hs[j].A, hs[j].plane, hs[j].nfluid, ctx->stream));
+            CK(lbm_init_lattice(precision, hs[j], ctx->stream));
             for (int t = 0; t < hs[j].ntiles; ++t) work.push_back(make_int2(j, t));
         }
         DevMem w(ctx->stream);
@@ -536,8 +571,7 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
         a.nwork = (int)work.size();
         auto launch = [&](long long s) {
             a.step = s;
-            return precision == LBM_FP64 ? launch_step3d_f64(v, dim3(a.nwork), ctx->stream, a)
-                                         : launch_step3d_lp(precision, v, true, dim3(a.nwork), ctx->stream, a);
+            return lbm_launch_step(precision, v, true, ((s + 1) & 1) == 1, dim3(a.nwork), ctx->stream, a);
         };
         long long s = 0;
         for (int i = 0; i < std::max(2, nsteps / 4); ++i) CK(launch(s++));

@@ -99,6 +99,7 @@ struct Solve3 {
     const uint32_t *wpre;    // pore voxels before each mask word (+ final total)
     const uint32_t *fnode;   // pore voxels, ascending linear index
     int nfluid;
+    int prec;                // LBM_FP64 .. LBM_M64
     int nx, ny, nz, wpr;
     long long nn;
     int ntiles;              // tiles of TPB*NPT pore voxels
@@ -290,47 +291,44 @@ __host__ __device__ constexpr int k_of(int dx, int dy, int dz)
 __device__ __forceinline__ void compact_nbrs(const Solve3 &S, unsigned i, int x, int y, int z, CNb &nb)
 {
     const int nx = S.nx, ny = S.ny, nz = S.nz, wpr = S.wpr;
+    const uint32_t *__restrict__ mask = S.mask;
+    const uint32_t *__restrict__ wpre = S.wpre;
     const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
     const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
     const int yr[3] = {ym, y, yp};
     const int zr[3] = {zm * ny, z * ny, zp * ny};
     const int b = x & 31, wx = x >> 5;
     const unsigned below = (1u << b) - 1u;
+    // words and bits of x - 1 and x + 1 within a row (periodic), and whether
+    // they leave the word of x: every lane takes the same instructions, the
+    // extra words are predicated loads (no divergent branches)
     const bool xlo = x == 0, xhi = x == nx - 1;
-    const int xm = xlo ? nx - 1 : x - 1;
+    const int xm = xlo ? nx - 1 : x - 1, xp = xhi ? 0 : x + 1;
+    const int wm = xm >> 5, bm = xm & 31, wp = xp >> 5, bp = xp & 31;
+    const bool om = wm != wx, op = wp != wx;
     unsigned bits = 0;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
         for (int dy = -1; dy <= 1; ++dy) {
-            const int row = zr[dz + 1] + yr[dy + 1];
-            const uint32_t *mrow = S.mask + (size_t)row * wpr;
-            const uint32_t *prow = S.wpre + (size_t)row * wpr;
-            const uint32_t m = __ldg(mrow + wx);
+            const unsigned rb = (unsigned)((zr[dz + 1] + yr[dy + 1]) * wpr);
+            const uint32_t m = __ldg(mask + rb + wx);
             const unsigned s0 = (m >> b) & 1u;
             const bool own = dy == 0 && dz == 0;
-            const unsigned A = own ? i : __ldg(prow + wx) + __popc(~m & below);
+            const unsigned A = own ? i : __ldg(wpre + rb + wx) + __popc(~m & below);
             if (!own) {
                 nb.idx[k_of(0, dy, dz)] = A;
                 bits |= s0 << k_of(0, dy, dz);
             }
             if (dy == 0 || dz == 0) {
                 const int km = k_of(-1, dy, dz), kp = k_of(1, dy, dz);
-                unsigned sm, im, sp, ip;
-                if (!xlo) {
-                    sm = b ? (m >> (b - 1)) & 1u : __ldg(mrow + wx - 1) >> 31;
-                    im = A - 1u;
-                } else {               // periodic: x - 1 is the last voxel of the row
-                    sm = (__ldg(mrow + (xm >> 5)) >> (xm & 31)) & 1u;
-                    im = __ldg(prow + wpr) - 1u;
-                }
-                if (!xhi) {
-                    sp = b != 31 ? (m >> (b + 1)) & 1u : __ldg(mrow + wx + 1) & 1u;
-                    ip = A + 1u - s0;
-                } else {               // periodic: x + 1 is the first voxel of the row
-                    sp = __ldg(mrow) & 1u;
-                    ip = __ldg(prow);
-                }
+                const uint32_t mmw = om ? __ldg(mask + rb + wm) : m;
+                const uint32_t mpw = op ? __ldg(mask + rb + wp) : m;
+                const unsigned sm = (mmw >> bm) & 1u, sp = (mpw >> bp) & 1u;
+                // rank of x - 1: A - 1, or the row's last pore across the wrap;
+                // rank of x + 1: A + (x is a pore), or the row's first pore
+                const unsigned im = xlo ? __ldg(wpre + rb + wpr) - 1u : A - 1u;
+                const unsigned ip = xhi ? __ldg(wpre + rb) : A + 1u - s0;
                 nb.idx[km] = im;
                 nb.idx[kp] = ip;
                 bits |= (sm << km) | (sp << kp);
@@ -347,19 +345,22 @@ __device__ __forceinline__ void coords3(const Solve3 &S, unsigned node, int &x, 
     y = r - z * S.ny;
 }
 
-// Step-kernel variants: (pore voxels per thread, resident blocks per SM the
-// register allocation is sized for).  More resident blocks put more loads in
-// flight but force spills; lbm_tune3d times them on the actual structure.
+// Step-kernel variants.  The two AA steps are separate kernels with separate
+// register budgets: the odd (local) step is pure streaming and wants many
+// loads in flight (several voxels per thread, high occupancy); the even
+// (neighbour) step carries the neighbour-rank arithmetic.  A variant index
+// v selects odd variant v / NVAR_EVEN and even variant v % NVAR_EVEN;
+// lbm_tune3d times them on the actual structure.
 struct Variant { int npt, minb; };
-constexpr int NVAR_LP = 4, NVAR_F64 = 3;
-__host__ __device__ constexpr Variant variant_lp(int v)
-{
-    return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : v == 2 ? Variant{2, 3} : Variant{2, 2};
-}
-__host__ __device__ constexpr Variant variant_f64(int v)
-{
-    return v == 0 ? Variant{1, 2} : v == 1 ? Variant{1, 1} : Variant{2, 1};
-}
+constexpr int NVAR_ODD = 3, NVAR_EVEN = 3;
+constexpr int NVAR_LP = NVAR_ODD * NVAR_EVEN, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
+__host__ __device__ constexpr Variant odd_lp(int v) { return v == 0 ? Variant{1, 4} : v == 1 ? Variant{1, 5} : Variant{2, 2}; }
+__host__ __device__ constexpr Variant even_lp(int v) { return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : Variant{1, 2}; }
+__host__ __device__ constexpr Variant odd_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{2, 1} : Variant{1, 1}; }
+__host__ __device__ constexpr Variant even_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{1, 1} : Variant{1, 3}; }
+// pore voxels per tile: the odd and even kernels of one solve share the tile
+// list (and its partials), so both use TPB * TILE_NPT voxels per tile
+constexpr int TILE_NPT = 2;
 
 // Collision dispatch: FP64 keeps the reference's arithmetic; reduced-precision
 // storage uses the pair-symmetric FP32 operator, specialised for tau = 1.
@@ -370,11 +371,58 @@ __device__ __forceinline__ void collide3(Cp (&g)[Q3], const Solve3 &S, Cp &ux, C
     else collide_ref64(g, S.P, ux, uy, uz);
 }
 
-// One thread per pore voxel of a tile: every lane does useful work whatever
-// the porosity, and every access is to a pore voxel's own compact slot or to
-// a neighbour's.
+// Odd (local) step: read A[k][i], collide, write A[opp k][i].  The NPT voxels
+// of a thread have all their loads issued before any store, so NPT x 19 loads
+// are in flight per thread.  One tile = TPB * TILE_NPT voxels.
 template <class ST, int NPT, int MINB, bool W1>
-__global__ void __launch_bounds__(TPB, MINB) step3d_kernel(const StepArgs a)
+__global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    using Cp = typename ST::C;
+    static_assert(TILE_NPT % NPT == 0, "tile must split evenly");
+    __shared__ double sh[TPB / 32][3];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S = a.solves[item.x];
+        const int phase = S.st->phase;
+        if (phase >= PH_DONE) continue;
+        const long long n = S.st->s_base + a.step + 1;
+        const bool red = needs_reduction(S.c, phase, n);
+        T *__restrict__ A = static_cast<T *>(S.A);
+        const unsigned P = (unsigned)S.plane;
+        double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int r = 0; r < TILE_NPT / NPT; ++r) {
+            unsigned iv[NPT];
+            bool vv[NPT];
+            Cp g[NPT][Q3];
+#pragma unroll
+            for (int j = 0; j < NPT; ++j) {
+                iv[j] = (unsigned)(item.y * (TPB * TILE_NPT) + (r * NPT + j) * TPB + threadIdx.x);
+                vv[j] = iv[j] < (unsigned)S.nfluid;
+#pragma unroll
+                for (int k = 0; k < Q3; ++k) g[j][k] = vv[j] ? ST::ld(A + (k * P + iv[j])) : Cp(0);
+            }
+#pragma unroll
+            for (int j = 0; j < NPT; ++j) {
+                if (!vv[j]) continue;
+                Cp ux, uy, uz;
+                collide3<ST, W1>(g[j], S, ux, uy, uz);
+#pragma unroll
+                for (int k = 0; k < Q3; ++k) ST::st(A + (opp3(k) * P + iv[j]), g[j][k]);
+                acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+            }
+        }
+        if (red) finish_tile(S, item.y, n, acc, sh);
+    }
+}
+
+// Even (neighbour) step: pull A[opp k][rank(x - e_k)] (A[k][i] across a solid
+// link), collide, push to A[k][rank(x + e_k)] (A[opp k][i] across a solid
+// link).  One voxel per thread at a time; a tile is TPB * TILE_NPT voxels.
+template <class ST, int MINB, bool W1>
+__global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a)
 {
     using T = typename ST::T;
     using Cp = typename ST::C;
@@ -385,44 +433,34 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_kernel(const StepArgs a)
         const Solve3 &S = a.solves[item.x];
         const int phase = S.st->phase;
         if (phase >= PH_DONE) continue;
-        const long long n = S.st->s_base + a.step + 1;          // this step's number
-        const bool neighbour = (n & 1ll) == 0;
+        const long long n = S.st->s_base + a.step + 1;
         const bool red = needs_reduction(S.c, phase, n);
         T *__restrict__ A = static_cast<T *>(S.A);
-        const unsigned P = (unsigned)S.plane;        // 19 * plane < 2^32 (checked on the host)
+        const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int j = 0; j < NPT; ++j) {
-            const unsigned i = (unsigned)(item.y * (TPB * NPT) + j * TPB + threadIdx.x);
+#pragma unroll 1
+        for (int j = 0; j < TILE_NPT; ++j) {
+            const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
             if (i >= (unsigned)S.nfluid) continue;
+            int x, y, z;
+            coords3(S, __ldg(S.fnode + i), x, y, z);
+            CNb nb;
+            compact_nbrs(S, i, x, y, z, nb);
             Cp g[Q3];
+            g[0] = ST::ld(A + i);
+#pragma unroll
+            for (int k = 1; k < Q3; ++k) {
+                const int o = opp3(k);
+                const unsigned src = ((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]);
+                g[k] = ST::ld(A + src);
+            }
             Cp ux, uy, uz;
-            if (!neighbour) {
+            collide3<ST, W1>(g, S, ux, uy, uz);
+            ST::st(A + i, g[0]);
 #pragma unroll
-                for (int k = 0; k < Q3; ++k) g[k] = ST::ld(A + (k * P + i));
-                collide3<ST, W1>(g, S, ux, uy, uz);
-#pragma unroll
-                for (int k = 0; k < Q3; ++k) ST::st(A + (opp3(k) * P + i), g[k]);
-            } else {
-                int x, y, z;
-                coords3(S, __ldg(S.fnode + i), x, y, z);
-                CNb nb;
-                compact_nbrs(S, i, x, y, z, nb);
-                g[0] = ST::ld(A + i);
-#pragma unroll
-                for (int k = 1; k < Q3; ++k) {
-                    // pull from x - e_k = x + e_opp(k); bounce back if that is solid
-                    const int o = opp3(k);
-                    const unsigned src = ((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]);
-                    g[k] = ST::ld(A + src);
-                }
-                collide3<ST, W1>(g, S, ux, uy, uz);
-                ST::st(A + i, g[0]);
-#pragma unroll
-                for (int k = 1; k < Q3; ++k) {
-                    const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                    ST::st(A + dst, g[k]);
-                }
+            for (int k = 1; k < Q3; ++k) {
+                const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
+                ST::st(A + dst, g[k]);
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
@@ -504,12 +542,16 @@ __global__ void canon3d_kernel(const Solve3 S, long long done, double *f_out, fl
 
 // Host-side launchers, one per translation unit (FP64 is compiled without FMA
 // contraction to keep the reference's rounding).
-cudaError_t launch_step3d_f64(int variant, dim3 grid, cudaStream_t s, const StepArgs &a);
-cudaError_t launch_step3d_lp(int prec, int variant, bool w1, dim3 grid, cudaStream_t s, const StepArgs &a);
+// `odd`: launch the odd-step (local) kernel, else the even-step one; every
+// solve in the launch must be at a step of that parity.
+cudaError_t launch_step3d_f64(int variant, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a);
+cudaError_t launch_step3d_lp(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a);
 cudaError_t launch_init3d(int prec, void *A, long long plane, long long n, cudaStream_t s);
 cudaError_t launch_canon3d(int prec, const Solve3 &S, long long done, double *f, float *u, cudaStream_t s);
-int max_blocks_step3d(int prec, int variant);
-inline int variant_count(int prec) { return prec == 0 ? NVAR_F64 : NVAR_LP; }
-inline int variant_npt(int prec, int v) { return prec == 0 ? variant_f64(v).npt : variant_lp(v).npt; }
+int max_blocks_step3d(int prec, int variant, bool odd);
+inline bool is_moment(int prec) { return prec == 4 || prec == 5; }
+inline int variant_count(int prec) { return prec == 0 ? NVAR_F64 : (prec >= 4 ? 3 : NVAR_LP); }
+// pore voxels per tile (in units of TPB) of a solve's tile list
+inline int variant_npt(int prec, int) { return prec >= 4 ? 1 : TILE_NPT; }
 
 }  // namespace lbm

@@ -48,7 +48,8 @@ struct lbm_batch {
     long long resident = 0;
     int cap_slots = 0;
     int cap_work = 0;
-    int grid = 0;
+    int grid = 0;          // persistent grid of the even-step (or moment) kernel
+    int grid_odd = 0;      // persistent grid of the odd-step kernel
     std::vector<Slot> slots;
     DevMem d_solves{nullptr}, d_states{nullptr}, d_work{nullptr}, d_nwork{nullptr};
     cudaGraph_t graph = nullptr;
@@ -77,10 +78,13 @@ static int capture(lbm_batch *b)
     a.nwork = 0;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
+    // chunks are even and solves join at chunk boundaries (s_base even), so
+    // launch i runs step i + 1 of every solve: odd launches use the local kernel
     for (int i = 0; i < b->chunk && e == cudaSuccess; ++i) {
         a.step = i;
-        e = b->precision == LBM_FP64 ? launch_step3d_f64(b->variant, dim3(b->grid), ctx->stream, a)
-                                     : launch_step3d_lp(b->precision, b->variant, b->w1, dim3(b->grid), ctx->stream, a);
+        const bool odd = ((i + 1) & 1) == 1;
+        a.nwork = 0;
+        e = lbm_launch_step(b->precision, b->variant, b->w1, odd, dim3(odd ? b->grid_odd : b->grid), ctx->stream, a);
     }
     if (e == cudaSuccess) {
         advance3d_kernel<<<(b->cap_slots + 255) / 256, 256, 0, ctx->stream>>>(
@@ -144,8 +148,9 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     if (!ctx || !out) return LBM_EINPUT;
     *out = nullptr;
     CK(cudaSetDevice(ctx->device));
-    if (precision < LBM_FP64 || precision > LBM_BF16) return lbm_fail_input(ctx, "unknown precision");
+    if (precision < LBM_FP64 || precision > LBM_M64) return lbm_fail_input(ctx, "unknown precision");
     if (chunk <= 0 || chunk > 4096) return lbm_fail_input(ctx, "chunk must be in 1..4096");
+    chunk += chunk & 1;                  // even: every solve keeps the launch's parity
     if (hbm_budget <= 0) return lbm_fail_input(ctx, "budget must be positive");
     std::unique_ptr<lbm_batch> b(new lbm_batch());
     b->ctx = ctx;
@@ -170,8 +175,8 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     std::vector<State3> done(b->cap_slots);
     for (auto &st : done) { memset(&st, 0, sizeof(st)); st.phase = PH_DONE; }
     CK(cudaMemcpyAsync(b->d_states.p, done.data(), sizeof(State3) * b->cap_slots, cudaMemcpyHostToDevice, ctx->stream));
-    const int per_sm = std::max(1, max_blocks_step3d(precision, b->variant));
-    b->grid = ctx->sms * per_sm;
+    b->grid = ctx->sms * std::max(1, lbm_max_blocks(precision, b->variant, false));
+    b->grid_odd = ctx->sms * std::max(1, lbm_max_blocks(precision, b->variant, true));
     int rc = sync_work(b.get());
     if (rc) return rc;
     rc = capture(b.get());
@@ -252,7 +257,7 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         s.retired = false;
         s.bytes = lbm_lattice_bytes3d(s.S.nfluid, b->precision) + 24ll * s.S.ntiles;
         lbm_init_state3(init[j], s.S.c);
-        CK(launch_init3d(b->precision, s.S.A, s.S.plane, s.S.nfluid, ctx->stream));
+        CK(lbm_init_lattice(b->precision, s.S, ctx->stream));
         CK(cudaMemcpyAsync(s.S.st, &init[j], sizeof(State3), cudaMemcpyHostToDevice, ctx->stream));
     }
     b->resident += exact;

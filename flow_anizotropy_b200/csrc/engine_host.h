@@ -63,3 +63,7 @@ int lbm_pick_npt(const lbm_params3d &p);
 // Pore-rank tables of a structure (wpre, fnode of S; nfluid, plane, ntiles for npt).
 int lbm_build_pores(lbm_ctx *ctx, lbm::Solve3 &S, int npt, DevMem &wpre, DevMem &fnode);
 void lbm_copy_pores(lbm::Solve3 &dst, const lbm::Solve3 &src);
+cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const lbm::StepArgs &a);
+int lbm_max_blocks(int prec, int variant, bool odd);
+cudaError_t lbm_init_lattice(int prec, const lbm::Solve3 &S, cudaStream_t s);
+cudaError_t lbm_canon(int prec, const lbm::Solve3 &S, long long done, double *f, float *u, cudaStream_t s);

@@ -5,23 +5,34 @@
 
 namespace lbm {
 
-#define LBM_F64(V) step3d_kernel<StoreF64, variant_f64(V).npt, variant_f64(V).minb, false>
+#define LBM_ODD(V) step3d_odd_kernel<StoreF64, odd_f64(V).npt, odd_f64(V).minb, false>
+#define LBM_EVEN(V) step3d_even_kernel<StoreF64, even_f64(V).minb, false>
 
-cudaError_t launch_step3d_f64(int variant, dim3 grid, cudaStream_t s, const StepArgs &a)
+cudaError_t launch_step3d_f64(int variant, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
-    switch (variant) {
-    case 0: LBM_F64(0)<<<grid, TPB, 0, s>>>(a); break;
-    case 1: LBM_F64(1)<<<grid, TPB, 0, s>>>(a); break;
-    case 2: LBM_F64(2)<<<grid, TPB, 0, s>>>(a); break;
-    default: return cudaErrorInvalidValue;
+    if (variant < 0 || variant >= NVAR_F64) return cudaErrorInvalidValue;
+    const int vo = variant / NVAR_EVEN, ve = variant % NVAR_EVEN;
+    if (odd) {
+        switch (vo) {
+        case 0: LBM_ODD(0)<<<grid, TPB, 0, s>>>(a); break;
+        case 1: LBM_ODD(1)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_ODD(2)<<<grid, TPB, 0, s>>>(a); break;
+        }
+    } else {
+        switch (ve) {
+        case 0: LBM_EVEN(0)<<<grid, TPB, 0, s>>>(a); break;
+        case 1: LBM_EVEN(1)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_EVEN(2)<<<grid, TPB, 0, s>>>(a); break;
+        }
     }
     return cudaGetLastError();
 }
 
-int max_blocks_f64(int variant)
+int max_blocks_f64(int variant, bool odd)
 {
-    const void *k = variant == 0 ? (const void *)LBM_F64(0) : variant == 1 ? (const void *)LBM_F64(1)
-                                                                           : (const void *)LBM_F64(2);
+    const int vo = variant / NVAR_EVEN, ve = variant % NVAR_EVEN;
+    const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(0) : vo == 1 ? (const void *)LBM_ODD(1) : (const void *)LBM_ODD(2))
+                        : (ve == 0 ? (const void *)LBM_EVEN(0) : ve == 1 ? (const void *)LBM_EVEN(1) : (const void *)LBM_EVEN(2));
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;

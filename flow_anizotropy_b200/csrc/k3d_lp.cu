@@ -6,50 +6,62 @@ namespace lbm {
 
 cudaError_t launch_init3d_f64(void *A, long long plane, long long n, cudaStream_t s);
 cudaError_t launch_canon3d_f64(const Solve3 &S, long long done, double *f, float *u, cudaStream_t s);
-int max_blocks_f64(int variant);
+int max_blocks_f64(int variant, bool odd);
 
-#define LBM_LP(ST, V, W) step3d_kernel<ST, variant_lp(V).npt, variant_lp(V).minb, W>
+#define LBM_ODD(ST, V, W) step3d_odd_kernel<ST, odd_lp(V).npt, odd_lp(V).minb, W>
+#define LBM_EVEN(ST, V, W) step3d_even_kernel<ST, even_lp(V).minb, W>
 
 template <class ST, bool W>
-static cudaError_t launch_lp(int v, dim3 grid, cudaStream_t s, const StepArgs &a)
+static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
-    switch (v) {
-    case 0: LBM_LP(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
-    case 1: LBM_LP(ST, 1, W)<<<grid, TPB, 0, s>>>(a); break;
-    case 2: LBM_LP(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
-    case 3: LBM_LP(ST, 3, W)<<<grid, TPB, 0, s>>>(a); break;
-    default: return cudaErrorInvalidValue;
+    if (v < 0 || v >= NVAR_LP) return cudaErrorInvalidValue;
+    const int vo = v / NVAR_EVEN, ve = v % NVAR_EVEN;
+    if (odd) {
+        switch (vo) {
+        case 0: LBM_ODD(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 1: LBM_ODD(ST, 1, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_ODD(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
+        }
+    } else {
+        switch (ve) {
+        case 0: LBM_EVEN(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 1: LBM_EVEN(ST, 1, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_EVEN(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
+        }
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_step3d_lp(int prec, int variant, bool w1, dim3 grid, cudaStream_t s, const StepArgs &a)
+cudaError_t launch_step3d_lp(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
     switch (prec) {
-    case 1: return w1 ? launch_lp<StoreF32, true>(variant, grid, s, a) : launch_lp<StoreF32, false>(variant, grid, s, a);
-    case 2: return w1 ? launch_lp<StoreF16, true>(variant, grid, s, a) : launch_lp<StoreF16, false>(variant, grid, s, a);
-    case 3: return w1 ? launch_lp<StoreBF16, true>(variant, grid, s, a) : launch_lp<StoreBF16, false>(variant, grid, s, a);
+    case 1: return w1 ? launch_lp<StoreF32, true>(variant, odd, grid, s, a) : launch_lp<StoreF32, false>(variant, odd, grid, s, a);
+    case 2: return w1 ? launch_lp<StoreF16, true>(variant, odd, grid, s, a) : launch_lp<StoreF16, false>(variant, odd, grid, s, a);
+    case 3: return w1 ? launch_lp<StoreBF16, true>(variant, odd, grid, s, a) : launch_lp<StoreBF16, false>(variant, odd, grid, s, a);
     default: return cudaErrorInvalidValue;
     }
 }
 
 template <class ST>
-static int occ(int v)
+static int occ(int v, bool odd)
 {
-    const void *k = v == 0 ? (const void *)LBM_LP(ST, 0, false) : v == 1 ? (const void *)LBM_LP(ST, 1, false)
-                  : v == 2 ? (const void *)LBM_LP(ST, 2, false) : (const void *)LBM_LP(ST, 3, false);
+    const int vo = v / NVAR_EVEN, ve = v % NVAR_EVEN;
+    const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(ST, 0, true) : vo == 1 ? (const void *)LBM_ODD(ST, 1, true)
+                                                                        : (const void *)LBM_ODD(ST, 2, true))
+                        : (ve == 0 ? (const void *)LBM_EVEN(ST, 0, true) : ve == 1 ? (const void *)LBM_EVEN(ST, 1, true)
+                                                                         : (const void *)LBM_EVEN(ST, 2, true));
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;
 }
 
-int max_blocks_step3d(int prec, int variant)
+int max_blocks_step3d(int prec, int variant, bool odd)
 {
     switch (prec) {
-    case 0: return max_blocks_f64(variant);
-    case 1: return occ<StoreF32>(variant);
-    case 2: return occ<StoreF16>(variant);
-    case 3: return occ<StoreBF16>(variant);
+    case 0: return max_blocks_f64(variant, odd);
+    case 1: return occ<StoreF32>(variant, odd);
+    case 2: return occ<StoreF16>(variant, odd);
+    case 3: return occ<StoreBF16>(variant, odd);
     default: return 0;
     }
 }

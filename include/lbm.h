@@ -47,6 +47,11 @@ extern "C" {
 #define LBM_FP32  1   /* shifted populations f_k - w_k as float                  */
 #define LBM_FP16  2   /* shifted populations, power-of-two scaled, IEEE half     */
 #define LBM_BF16  3   /* shifted populations as bfloat16                         */
+/* tau = 1 only: the post-collision populations are a function of a voxel's
+ * moments, so the state is (rho - 1, u) per pore voxel (exact reformulation;
+ * rounding at the storage precision). */
+#define LBM_M32   4   /* moments as float, FP32 arithmetic                       */
+#define LBM_M64   5   /* moments as double, FP64 arithmetic                      */
 
 /* Phase-1 convergence criterion */
 #define LBM_CRIT_DRIFT  0  /* every lag steps: max_c |q_c - qprev_c| < eps ||q||
