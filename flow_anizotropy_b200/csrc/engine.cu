@@ -176,6 +176,14 @@ long long lbm_plane_for(int prec, long long n)
     return is_moment(prec) ? mom_buffer_elems(prec, n) : lbm_plane_elems(n);
 }
 
+// A variant whose even kernel reads neighbour records needs them built.
+int lbm_effective_variant(int prec, int variant, bool have_meta)
+{
+    if (is_moment(prec) || have_meta) return variant;
+    const int ve = variant % NVAR_EVEN;
+    return even_meta(ve) ? variant + 2 : variant;      // same budget, ranks from the mask
+}
+
 cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
     if (prec == LBM_FP64) return launch_step3d_f64(variant, odd, grid, s, a);
@@ -251,7 +259,7 @@ void lbm_init_state3(State3 &st, const Ctl3 &c)
 
 int lbm_pick_npt(const lbm_params3d &p) { return variant_npt(p.precision, p.variant); }
 
-int lbm_build_pores(lbm_ctx *ctx, Solve3 &S, int npt, DevMem &wpre, DevMem &fnode)
+int lbm_build_pores(lbm_ctx *ctx, Solve3 &S, int npt, DevMem &wpre, DevMem &fnode, DevMem &meta, DevMem &meta2)
 {
     const long long nwords = (long long)S.wpr * S.ny * S.nz;
     const int blocks = (int)((nwords + SCAN_WORDS - 1) / SCAN_WORDS);
@@ -285,12 +293,26 @@ int lbm_build_pores(lbm_ctx *ctx, Solve3 &S, int npt, DevMem &wpre, DevMem &fnod
     S.plane = lbm_plane_for(S.prec, (long long)total);
     S.ntiles = (int)((total + (unsigned long long)TPB * npt - 1) / ((unsigned long long)TPB * npt));
     if (S.ntiles == 0) S.ntiles = 1;
+    S.meta = nullptr;
+    S.meta2 = nullptr;
+    // neighbour records (24 B per pore voxel) for the even-step kernels that
+    // read them; in-row offsets are 16-bit, so rows up to 65535 voxels
+    if (!is_moment(S.prec) && S.nx <= 65535 && total > 0) {
+        CK(meta.alloc(sizeof(uint4) * (size_t)total));
+        CK(meta2.alloc(sizeof(uint2) * (size_t)total));
+        const int mb = (int)std::min<unsigned long long>((total + 255) / 256, 8ull * 1184);
+        build_meta_kernel<<<mb, 256, 0, ctx->stream>>>(S, static_cast<uint4 *>(meta.p), static_cast<uint2 *>(meta2.p));
+        CK(cudaGetLastError());
+        S.meta = static_cast<const uint4 *>(meta.p);
+        S.meta2 = static_cast<const uint2 *>(meta2.p);
+    }
     return LBM_OK;
 }
 
 void lbm_copy_pores(Solve3 &dst, const Solve3 &src)
 {
     dst.wpre = src.wpre; dst.fnode = src.fnode; dst.nfluid = src.nfluid;
+    dst.meta = src.meta; dst.meta2 = src.meta2;
     dst.plane = src.plane; dst.ntiles = src.ntiles;
 }
 
@@ -303,6 +325,7 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
     const int n = (int)hs.size();
     bool w1 = true;
     for (const Solve3 &S : hs) w1 = w1 && S.P.tau == 1.0;
+    variant = lbm_effective_variant(prec, variant, hs.empty() || hs[0].meta != nullptr);
     long long s = 0;
     StepArgs a;
     a.solves = d_solves; a.work = d_work; a.nwork_dev = nullptr; a.nwork = nwork;
@@ -358,11 +381,11 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
     std::vector<DevMem> lat, part;
     lat.reserve(ndir); part.reserve(ndir);
     DevMem d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream);
-    DevMem wpre(ctx->stream), fnode(ctx->stream);
+    DevMem wpre(ctx->stream), fnode(ctx->stream), meta(ctx->stream), meta2(ctx->stream);
     Solve3 proto;
     lbm_fill_solve3(proto, nx, ny, nz, forces, p, npt);
     proto.mask = static_cast<const uint32_t *>(mask.p);
-    rc = lbm_build_pores(ctx, proto, npt, wpre, fnode);
+    rc = lbm_build_pores(ctx, proto, npt, wpre, fnode, meta, meta2);
     if (rc) return rc;
     CK(d_states.alloc(sizeof(State3) * ndir));
     for (int j = 0; j < ndir; ++j) {
@@ -454,9 +477,9 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     Solve3 &S = hs[0];
     lbm_fill_solve3(S, nx, ny, nz, force, p, npt);
     DevMem lat(ctx->stream), part(ctx->stream), d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream);
-    DevMem wpre(ctx->stream), fnode(ctx->stream);
+    DevMem wpre(ctx->stream), fnode(ctx->stream), meta(ctx->stream), meta2(ctx->stream);
     S.mask = static_cast<const uint32_t *>(mask.p);
-    rc = lbm_build_pores(ctx, S, npt, wpre, fnode);
+    rc = lbm_build_pores(ctx, S, npt, wpre, fnode, meta, meta2);
     if (rc) return rc;
     CK(lat.alloc((size_t)lbm_lattice_bytes3d(S.nfluid, precision)));
     CK(part.alloc(sizeof(double) * 3 * (size_t)S.ntiles));
@@ -536,12 +559,12 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
         p.tau = 1.0; p.lag = LLONG_MAX / 4; p.hold = 1 << 30; p.max_steps = LLONG_MAX / 4;
         p.precision = precision; p.variant = v; p.sample = 1;
         const int npt = variant_npt(precision, v);
-        DevMem wpre(ctx->stream), fnode(ctx->stream);
+        DevMem wpre(ctx->stream), fnode(ctx->stream), meta(ctx->stream), meta2(ctx->stream);
         Solve3 proto;
         const double F0[3] = {1e-6, 0, 0};
         lbm_fill_solve3(proto, nx, ny, nz, F0, p, npt);
         proto.mask = static_cast<const uint32_t *>(mask.p);
-        rc = lbm_build_pores(ctx, proto, npt, wpre, fnode);
+        rc = lbm_build_pores(ctx, proto, npt, wpre, fnode, meta, meta2);
         if (rc) break;
         std::vector<Solve3> hs(ndir);
         std::vector<State3> hst(ndir);
@@ -569,9 +592,10 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
         a.work = static_cast<const int2 *>(w.p);
         a.nwork_dev = nullptr;
         a.nwork = (int)work.size();
+        const int ev = lbm_effective_variant(precision, v, proto.meta != nullptr);
         auto launch = [&](long long s) {
             a.step = s;
-            return lbm_launch_step(precision, v, true, ((s + 1) & 1) == 1, dim3(a.nwork), ctx->stream, a);
+            return lbm_launch_step(precision, ev, true, ((s + 1) & 1) == 1, dim3(a.nwork), ctx->stream, a);
         };
         long long s = 0;
         for (int i = 0; i < std::max(2, nsteps / 4); ++i) CK(launch(s++));

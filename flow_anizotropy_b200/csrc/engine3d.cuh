@@ -98,6 +98,8 @@ struct Solve3 {
     const uint32_t *mask;
     const uint32_t *wpre;    // pore voxels before each mask word (+ final total)
     const uint32_t *fnode;   // pore voxels, ascending linear index
+    const uint4 *meta;       // per pore voxel: neighbour record (see NbMeta), or null
+    const uint2 *meta2;
     int nfluid;
     int prec;                // LBM_FP64 .. LBM_M64
     int nx, ny, nz, wpr;
@@ -345,6 +347,58 @@ __device__ __forceinline__ void coords3(const Solve3 &S, unsigned node, int &x, 
     y = r - z * S.ny;
 }
 
+// Per-pore-voxel neighbour record, built once per structure, so that the even
+// step gets its 18 neighbour ranks from 24 bytes and a few table reads
+// instead of the mask arithmetic of compact_nbrs:
+//   meta.x  row index r = z*ny + y of the voxel
+//   meta.y  bits 0-18: x + e_k solid; 19/20: x == 0 / nx-1; 21/22: y == 0 /
+//           ny-1; 23/24: z == 0 / nz-1
+//   meta.z  pores before x in rows (y-1, z) | (y+1, z) << 16
+//   meta.w  pores before x in rows (y, z-1) | (y, z+1) << 16
+//   meta2.x pores before x in rows (y-1, z-1) | (y+1, z-1) << 16
+//   meta2.y pores before x in rows (y-1, z+1) | (y+1, z+1) << 16
+// The rank of (x, row') is rowstart(row') + offset with rowstart(r) =
+// wpre[r * wpr]; x +- 1 ranks follow from the row's rank at x and the solid
+// bits, or across the periodic x wrap from the row's first / last pore.
+constexpr unsigned LK_XLO = 1u << 19, LK_XHI = 1u << 20, LK_YLO = 1u << 21, LK_YHI = 1u << 22,
+                   LK_ZLO = 1u << 23, LK_ZHI = 1u << 24;
+
+__device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, CNb &nb)
+{
+    const uint4 m = __ldg(S.meta + i);
+    const uint2 m2 = __ldg(S.meta2 + i);
+    const int ny = S.ny, nz = S.nz, wpr = S.wpr;
+    const uint32_t *__restrict__ wpre = S.wpre;
+    const int row = (int)m.x;
+    const unsigned link = m.y;
+    const bool xlo = link & LK_XLO, xhi = link & LK_XHI;
+    const int dym = (link & LK_YLO) ? ny - 1 : -1, dyp = (link & LK_YHI) ? 1 - ny : 1;
+    const int dzm = (link & LK_ZLO) ? (nz - 1) * ny : -ny, dzp = (link & LK_ZHI) ? -(nz - 1) * ny : ny;
+    const int rows[3][3] = {{row + dzm + dym, row + dym, row + dzp + dym},
+                            {row + dzm, row, row + dzp},
+                            {row + dzm + dyp, row + dyp, row + dzp + dyp}};   // [dy+1][dz+1]
+    const unsigned offs[3][3] = {{m2.x & 0xffffu, m.z & 0xffffu, m2.y & 0xffffu},
+                                 {m.w & 0xffffu, 0u, m.w >> 16},
+                                 {m2.x >> 16, m.z >> 16, m2.y >> 16}};
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+            const bool own = dy == 0 && dz == 0;
+            const int r = rows[dy + 1][dz + 1];
+            const bool face = dy == 0 || dz == 0;
+            const unsigned rs = (!own || xhi) ? __ldg(wpre + (unsigned)r * wpr) : 0u;
+            const unsigned A = own ? i : rs + offs[dy + 1][dz + 1];
+            if (!own) nb.idx[k_of(0, dy, dz)] = A;
+            if (face) {
+                const unsigned s0 = own ? 0u : (link >> k_of(0, dy, dz)) & 1u;
+                nb.idx[k_of(-1, dy, dz)] = xlo ? __ldg(wpre + (unsigned)(r + 1) * wpr) - 1u : A - 1u;
+                nb.idx[k_of(1, dy, dz)] = xhi ? rs : A + 1u - s0;
+            }
+        }
+    nb.solid = link & 0x7ffffu;
+}
+
 // Step-kernel variants.  The two AA steps are separate kernels with separate
 // register budgets: the odd (local) step is pure streaming and wants many
 // loads in flight (several voxels per thread, high occupancy); the even
@@ -352,12 +406,14 @@ __device__ __forceinline__ void coords3(const Solve3 &S, unsigned node, int &x, 
 // v selects odd variant v / NVAR_EVEN and even variant v % NVAR_EVEN;
 // lbm_tune3d times them on the actual structure.
 struct Variant { int npt, minb; };
-constexpr int NVAR_ODD = 3, NVAR_EVEN = 3;
+constexpr int NVAR_ODD = 3, NVAR_EVEN = 4;
 constexpr int NVAR_LP = NVAR_ODD * NVAR_EVEN, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
 __host__ __device__ constexpr Variant odd_lp(int v) { return v == 0 ? Variant{1, 4} : v == 1 ? Variant{1, 5} : Variant{2, 2}; }
-__host__ __device__ constexpr Variant even_lp(int v) { return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : Variant{1, 2}; }
+// even variants: 0-1 read the neighbour record (META), 2-3 compute ranks from the mask
+__host__ __device__ constexpr Variant even_lp(int v) { return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : v == 2 ? Variant{1, 3} : Variant{1, 4}; }
+__host__ __device__ constexpr bool even_meta(int v) { return v < 2; }
 __host__ __device__ constexpr Variant odd_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{2, 1} : Variant{1, 1}; }
-__host__ __device__ constexpr Variant even_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{1, 1} : Variant{1, 3}; }
+__host__ __device__ constexpr Variant even_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{1, 1} : v == 2 ? Variant{1, 2} : Variant{1, 1}; }
 // pore voxels per tile: the odd and even kernels of one solve share the tile
 // list (and its partials), so both use TPB * TILE_NPT voxels per tile
 constexpr int TILE_NPT = 2;
@@ -421,7 +477,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
 // Even (neighbour) step: pull A[opp k][rank(x - e_k)] (A[k][i] across a solid
 // link), collide, push to A[k][rank(x + e_k)] (A[opp k][i] across a solid
 // link).  One voxel per thread at a time; a tile is TPB * TILE_NPT voxels.
-template <class ST, int MINB, bool W1>
+template <class ST, int MINB, bool W1, bool META>
 __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a)
 {
     using T = typename ST::T;
@@ -442,10 +498,14 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
         for (int j = 0; j < TILE_NPT; ++j) {
             const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
             if (i >= (unsigned)S.nfluid) continue;
-            int x, y, z;
-            coords3(S, __ldg(S.fnode + i), x, y, z);
             CNb nb;
-            compact_nbrs(S, i, x, y, z, nb);
+            if constexpr (META) {
+                meta_nbrs(S, i, nb);
+            } else {
+                int x, y, z;
+                coords3(S, __ldg(S.fnode + i), x, y, z);
+                compact_nbrs(S, i, x, y, z, nb);
+            }
             Cp g[Q3];
             g[0] = ST::ld(A + i);
 #pragma unroll
@@ -474,6 +534,7 @@ __global__ void word_sums_kernel(const uint32_t *mask, long long nwords, unsigne
 __global__ void word_scan_kernel(const uint32_t *mask, long long nwords, const unsigned *boff, uint32_t *wpre);
 __global__ void scatter_fnode_kernel(const uint32_t *mask, const uint32_t *wpre, long long nwords, int wpr,
                                      int nx, uint32_t *fnode);
+__global__ void build_meta_kernel(Solve3 S, uint4 *meta, uint2 *meta2);
 
 // After a chunk of `steps` launches, solves still running have advanced by it.
 __global__ void advance3d_kernel(Solve3 *solves, int nsolves, long long steps);

@@ -28,7 +28,7 @@ struct Slot {
     int dir = 0;
     Solve3 S{};
     std::shared_ptr<DevMem> mask;     // shared by the directions of one structure
-    std::shared_ptr<DevMem> wpre, fnode;
+    std::shared_ptr<DevMem> wpre, fnode, meta, meta2;
     DevMem lattice{nullptr};
     DevMem partials{nullptr};
     long long bytes = 0;
@@ -138,7 +138,7 @@ extern "C" long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int pre
 {
     const long long nn = (long long)nx * ny * nz;
     // upper bound: every voxel a pore (the batch charges the exact size on admission)
-    const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 4ll * nn + 8;
+    const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 28ll * nn + 8;
     const long long tiles = (nn + TPB - 1) / TPB;
     return tables + (long long)ndir * (lbm_lattice_bytes3d(nn, precision) + 24 * tiles);
 }
@@ -220,12 +220,20 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
     rc = lbm_upload_mask(ctx, solid, nx, (long long)ny * nz, *mask, npore);
     if (rc) return rc;
     auto wpre = std::make_shared<DevMem>(ctx->stream), fnode = std::make_shared<DevMem>(ctx->stream);
+    auto meta = std::make_shared<DevMem>(ctx->stream), meta2 = std::make_shared<DevMem>(ctx->stream);
     Solve3 proto;
     lbm_fill_solve3(proto, nx, ny, nz, forces, p, b->npt);
     proto.mask = static_cast<const uint32_t *>(mask->p);
-    rc = lbm_build_pores(ctx, proto, b->npt, *wpre, *fnode);
+    rc = lbm_build_pores(ctx, proto, b->npt, *wpre, *fnode, *meta, *meta2);
     if (rc) return rc;
-    const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 4ll * proto.nfluid + 8;
+    if (!proto.meta && lbm_effective_variant(b->precision, b->variant, false) != b->variant) {
+        // a structure too wide for neighbour records: the batch computes ranks
+        b->variant = lbm_effective_variant(b->precision, b->variant, false);
+        rc = capture(b);
+        if (rc) return rc;
+    }
+    const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 4ll * proto.nfluid + 8 +
+                             (proto.meta ? 24ll * proto.nfluid : 0);
     const long long exact = tables + (long long)ndir * (lbm_lattice_bytes3d(proto.nfluid, b->precision) + 24ll * proto.ntiles);
     if (b->resident + exact > b->budget) {
         ctx->err = "batch budget exhausted";
@@ -242,7 +250,7 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         Slot &s = b->slots[free_slots[j]];
         lbm_fill_solve3(s.S, nx, ny, nz, forces + 3 * j, p, b->npt);
         lbm_copy_pores(s.S, proto);
-        s.wpre = wpre; s.fnode = fnode;
+        s.wpre = wpre; s.fnode = fnode; s.meta = meta; s.meta2 = meta2;
         s.tables = tables;
         CK(s.lattice.alloc((size_t)lbm_lattice_bytes3d(s.S.nfluid, b->precision)));
         CK(s.partials.alloc(sizeof(double) * 3 * (size_t)s.S.ntiles));
@@ -306,6 +314,8 @@ extern "C" int lbm_batch_poll(lbm_batch *b, long long *tags, int *dirs, lbm_resu
         s.mask.reset();
         s.wpre.reset();
         s.fnode.reset();
+        s.meta.reset();
+        s.meta2.reset();
         changed = true;
     }
     if (changed) return sync_work(b);

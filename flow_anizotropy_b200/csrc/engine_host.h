@@ -61,7 +61,9 @@ void lbm_fill_solve3(lbm::Solve3 &S, int nx, int ny, int nz, const double F[3], 
 void lbm_init_state3(lbm::State3 &st, const lbm::Ctl3 &c);
 int lbm_pick_npt(const lbm_params3d &p);
 // Pore-rank tables of a structure (wpre, fnode of S; nfluid, plane, ntiles for npt).
-int lbm_build_pores(lbm_ctx *ctx, lbm::Solve3 &S, int npt, DevMem &wpre, DevMem &fnode);
+int lbm_build_pores(lbm_ctx *ctx, lbm::Solve3 &S, int npt, DevMem &wpre, DevMem &fnode, DevMem &meta,
+                    DevMem &meta2);
+int lbm_effective_variant(int prec, int variant, bool have_meta);
 void lbm_copy_pores(lbm::Solve3 &dst, const lbm::Solve3 &src);
 cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const lbm::StepArgs &a);
 int lbm_max_blocks(int prec, int variant, bool odd);

@@ -6,7 +6,7 @@
 namespace lbm {
 
 #define LBM_ODD(V) step3d_odd_kernel<StoreF64, odd_f64(V).npt, odd_f64(V).minb, false>
-#define LBM_EVEN(V) step3d_even_kernel<StoreF64, even_f64(V).minb, false>
+#define LBM_EVEN(V) step3d_even_kernel<StoreF64, even_f64(V).minb, false, even_meta(V)>
 
 cudaError_t launch_step3d_f64(int variant, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
@@ -22,7 +22,8 @@ cudaError_t launch_step3d_f64(int variant, bool odd, dim3 grid, cudaStream_t s, 
         switch (ve) {
         case 0: LBM_EVEN(0)<<<grid, TPB, 0, s>>>(a); break;
         case 1: LBM_EVEN(1)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_EVEN(2)<<<grid, TPB, 0, s>>>(a); break;
+        case 2: LBM_EVEN(2)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_EVEN(3)<<<grid, TPB, 0, s>>>(a); break;
         }
     }
     return cudaGetLastError();
@@ -32,7 +33,8 @@ int max_blocks_f64(int variant, bool odd)
 {
     const int vo = variant / NVAR_EVEN, ve = variant % NVAR_EVEN;
     const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(0) : vo == 1 ? (const void *)LBM_ODD(1) : (const void *)LBM_ODD(2))
-                        : (ve == 0 ? (const void *)LBM_EVEN(0) : ve == 1 ? (const void *)LBM_EVEN(1) : (const void *)LBM_EVEN(2));
+                        : (ve == 0 ? (const void *)LBM_EVEN(0) : ve == 1 ? (const void *)LBM_EVEN(1)
+                           : ve == 2 ? (const void *)LBM_EVEN(2) : (const void *)LBM_EVEN(3));
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;

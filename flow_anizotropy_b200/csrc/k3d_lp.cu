@@ -9,7 +9,7 @@ cudaError_t launch_canon3d_f64(const Solve3 &S, long long done, double *f, float
 int max_blocks_f64(int variant, bool odd);
 
 #define LBM_ODD(ST, V, W) step3d_odd_kernel<ST, odd_lp(V).npt, odd_lp(V).minb, W>
-#define LBM_EVEN(ST, V, W) step3d_even_kernel<ST, even_lp(V).minb, W>
+#define LBM_EVEN(ST, V, W) step3d_even_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 
 template <class ST, bool W>
 static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
@@ -26,7 +26,8 @@ static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const S
         switch (ve) {
         case 0: LBM_EVEN(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
         case 1: LBM_EVEN(ST, 1, W)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_EVEN(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 2: LBM_EVEN(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_EVEN(ST, 3, W)<<<grid, TPB, 0, s>>>(a); break;
         }
     }
     return cudaGetLastError();
@@ -49,7 +50,7 @@ static int occ(int v, bool odd)
     const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(ST, 0, true) : vo == 1 ? (const void *)LBM_ODD(ST, 1, true)
                                                                         : (const void *)LBM_ODD(ST, 2, true))
                         : (ve == 0 ? (const void *)LBM_EVEN(ST, 0, true) : ve == 1 ? (const void *)LBM_EVEN(ST, 1, true)
-                                                                         : (const void *)LBM_EVEN(ST, 2, true));
+                           : ve == 2 ? (const void *)LBM_EVEN(ST, 2, true) : (const void *)LBM_EVEN(ST, 3, true));
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;
@@ -157,6 +158,33 @@ __global__ void scatter_fnode_kernel(const uint32_t *mask, const uint32_t *wpre,
             f &= f - 1u;
             fnode[at++] = (uint32_t)(row * nx + x0 + b);
         }
+    }
+}
+
+// Neighbour records of every pore voxel (see meta_nbrs).
+__global__ void build_meta_kernel(Solve3 S, uint4 *meta, uint2 *meta2)
+{
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < (unsigned)S.nfluid;
+         i += gridDim.x * blockDim.x) {
+        int x, y, z;
+        coords3(S, S.fnode[i], x, y, z);
+        CNb nb;
+        compact_nbrs(S, i, x, y, z, nb);
+        const int ny = S.ny, nz = S.nz, wpr = S.wpr;
+        const int row = z * ny + y;
+        const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+        const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
+        auto off = [&](int yy, int zz, int k) -> unsigned {
+            return nb.idx[k] - S.wpre[(unsigned)(zz * ny + yy) * wpr];
+        };
+        unsigned link = nb.solid & 0x7ffffu;
+        link |= (x == 0 ? LK_XLO : 0u) | (x == S.nx - 1 ? LK_XHI : 0u) | (y == 0 ? LK_YLO : 0u) |
+                (y == ny - 1 ? LK_YHI : 0u) | (z == 0 ? LK_ZLO : 0u) | (z == nz - 1 ? LK_ZHI : 0u);
+        meta[i] = make_uint4((unsigned)row, link,
+                             off(ym, z, k_of(0, -1, 0)) | (off(yp, z, k_of(0, 1, 0)) << 16),
+                             off(y, zm, k_of(0, 0, -1)) | (off(y, zp, k_of(0, 0, 1)) << 16));
+        meta2[i] = make_uint2(off(ym, zm, k_of(0, -1, -1)) | (off(yp, zm, k_of(0, 1, -1)) << 16),
+                              off(ym, zp, k_of(0, -1, 1)) | (off(yp, zp, k_of(0, 1, 1)) << 16));
     }
 }
 
