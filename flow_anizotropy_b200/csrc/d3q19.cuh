@@ -182,36 +182,59 @@ __device__ __forceinline__ void collide_pairs(float (&h)[Q3], const Phys3 &P, fl
 // Storage formats: element type, compute type, whether the stored value is
 // the (scaled) shifted population, and plain load/store conversions.
 // ---------------------------------------------------------------------------
+// W: the word cp.async stages for one population (cp.async copies 4, 8 or 16
+// bytes, so a 2-byte population travels in the aligned 4-byte word that
+// holds it, and `unword` picks its half).
 struct StoreF64 {
-    using T = double; using C = double;
+    using T = double; using C = double; using W = double;
+    __device__ static __forceinline__ const W *word(const T *p) { return p; }
+    __device__ static __forceinline__ C unword(W w, unsigned) { return w; }
     static constexpr bool shifted = false;
     static constexpr int code = 0;
-    __device__ static __forceinline__ C ld(const T *p) { return *p; }
-    __device__ static __forceinline__ void st(T *p, C v) { *p = v; }
+    __device__ static __forceinline__ C ld(const T *p) { return __ldcs(p); }
+    __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, v); }
     __host__ __device__ static constexpr double init(int k) { return w3(k); }
 };
 struct StoreF32 {
-    using T = float; using C = float;
+    using T = float; using C = float; using W = float;
+    __device__ static __forceinline__ const W *word(const T *p) { return p; }
+    __device__ static __forceinline__ C unword(W w, unsigned) { return w; }
     static constexpr bool shifted = true;
     static constexpr int code = 1;
-    __device__ static __forceinline__ C ld(const T *p) { return *p; }
-    __device__ static __forceinline__ void st(T *p, C v) { *p = v; }
+    __device__ static __forceinline__ C ld(const T *p) { return __ldcs(p); }
+    __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, v); }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 struct StoreF16 {
-    using T = __half; using C = float;
+    using T = __half; using C = float; using W = uint32_t;
+    __device__ static __forceinline__ const W *word(const T *p)
+    {
+        return reinterpret_cast<const W *>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3));
+    }
+    __device__ static __forceinline__ C unword(W w, unsigned idx)
+    {
+        return __half2float(__ushort_as_half((unsigned short)(w >> ((idx & 1u) * 16))));
+    }
     static constexpr bool shifted = true;
     static constexpr int code = 2;
-    __device__ static __forceinline__ C ld(const T *p) { return __half2float(*p); }
-    __device__ static __forceinline__ void st(T *p, C v) { *p = __float2half_rn(v); }
+    __device__ static __forceinline__ C ld(const T *p) { return __half2float(__ldcs(p)); }
+    __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, __float2half_rn(v)); }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 struct StoreBF16 {
-    using T = __nv_bfloat16; using C = float;
+    using T = __nv_bfloat16; using C = float; using W = uint32_t;
+    __device__ static __forceinline__ const W *word(const T *p)
+    {
+        return reinterpret_cast<const W *>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3));
+    }
+    __device__ static __forceinline__ C unword(W w, unsigned idx)
+    {
+        return __bfloat162float(__ushort_as_bfloat16((unsigned short)(w >> ((idx & 1u) * 16))));
+    }
     static constexpr bool shifted = true;
     static constexpr int code = 3;
-    __device__ static __forceinline__ C ld(const T *p) { return __bfloat162float(*p); }
-    __device__ static __forceinline__ void st(T *p, C v) { *p = __float2bfloat16_rn(v); }
+    __device__ static __forceinline__ C ld(const T *p) { return __bfloat162float(__ldcs(p)); }
+    __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, __float2bfloat16_rn(v)); }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 

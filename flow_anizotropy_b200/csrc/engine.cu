@@ -181,7 +181,8 @@ int lbm_effective_variant(int prec, int variant, bool have_meta)
 {
     if (is_moment(prec) || have_meta) return variant;
     const int ve = variant % NVAR_EVEN;
-    return even_meta(ve) ? variant + 2 : variant;      // same budget, ranks from the mask
+    if (!even_meta(ve)) return variant;
+    return variant - ve + (ve & 1) + 2;                 // same budget, ranks from the mask
 }
 
 cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
@@ -297,7 +298,7 @@ int lbm_build_pores(lbm_ctx *ctx, Solve3 &S, int npt, DevMem &wpre, DevMem &fnod
     S.meta2 = nullptr;
     // neighbour records (24 B per pore voxel) for the even-step kernels that
     // read them; in-row offsets are 16-bit, so rows up to 65535 voxels
-    if (!is_moment(S.prec) && S.nx <= 65535 && total > 0) {
+    if (S.nx <= 65535 && total > 0) {
         CK(meta.alloc(sizeof(uint4) * (size_t)total));
         CK(meta2.alloc(sizeof(uint2) * (size_t)total));
         const int mb = (int)std::min<unsigned long long>((total + 255) / 256, 8ull * 1184);

@@ -29,6 +29,7 @@
 // each at its own step number, so solves admitted at different times share a
 // launch.
 #pragma once
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -363,10 +364,8 @@ __device__ __forceinline__ void coords3(const Solve3 &S, unsigned node, int &x, 
 constexpr unsigned LK_XLO = 1u << 19, LK_XHI = 1u << 20, LK_YLO = 1u << 21, LK_YHI = 1u << 22,
                    LK_ZLO = 1u << 23, LK_ZHI = 1u << 24;
 
-__device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, CNb &nb)
+__device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, const uint4 m, const uint2 m2, CNb &nb)
 {
-    const uint4 m = __ldg(S.meta + i);
-    const uint2 m2 = __ldg(S.meta2 + i);
     const int ny = S.ny, nz = S.nz, wpr = S.wpr;
     const uint32_t *__restrict__ wpre = S.wpre;
     const int row = (int)m.x;
@@ -406,14 +405,24 @@ __device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, CNb &nb)
 // v selects odd variant v / NVAR_EVEN and even variant v % NVAR_EVEN;
 // lbm_tune3d times them on the actual structure.
 struct Variant { int npt, minb; };
-constexpr int NVAR_ODD = 3, NVAR_EVEN = 4;
+constexpr int NVAR_ODD = 3, NVAR_EVEN = 6;
 constexpr int NVAR_LP = NVAR_ODD * NVAR_EVEN, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
 __host__ __device__ constexpr Variant odd_lp(int v) { return v == 0 ? Variant{1, 4} : v == 1 ? Variant{1, 5} : Variant{2, 2}; }
-// even variants: 0-1 read the neighbour record (META), 2-3 compute ranks from the mask
-__host__ __device__ constexpr Variant even_lp(int v) { return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : v == 2 ? Variant{1, 3} : Variant{1, 4}; }
-__host__ __device__ constexpr bool even_meta(int v) { return v < 2; }
+// even variants: 0-1 read the neighbour record (META), 2-3 compute ranks from
+// the mask, 4-5 read the record and stage their gathers with cp.async
+__host__ __device__ constexpr Variant even_lp(int v)
+{
+    return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : v == 2 ? Variant{1, 3} : v == 3 ? Variant{1, 4}
+         : v == 4 ? Variant{1, 4} : Variant{1, 3};
+}
+__host__ __device__ constexpr bool even_meta(int v) { return v < 2 || v >= 4; }
+__host__ __device__ constexpr bool even_async(int v) { return v >= 4; }
 __host__ __device__ constexpr Variant odd_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{2, 1} : Variant{1, 1}; }
-__host__ __device__ constexpr Variant even_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{1, 1} : v == 2 ? Variant{1, 2} : Variant{1, 1}; }
+__host__ __device__ constexpr Variant even_f64(int v)
+{
+    return v == 0 ? Variant{1, 2} : v == 1 ? Variant{1, 1} : v == 2 ? Variant{1, 2} : v == 3 ? Variant{1, 1}
+         : v == 4 ? Variant{1, 2} : Variant{1, 3};
+}
 // pore voxels per tile: the odd and even kernels of one solve share the tile
 // list (and its partials), so both use TPB * TILE_NPT voxels per tile
 constexpr int TILE_NPT = 2;
@@ -494,13 +503,27 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
         T *__restrict__ A = static_cast<T *>(S.A);
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
-#pragma unroll 1
+        // the records of all of this thread's voxels are requested up front:
+        // each voxel's chain (record -> row starts -> populations) then starts
+        // with its first DRAM trip already under way
+        uint4 mr[TILE_NPT];
+        uint2 mr2[TILE_NPT];
+        if constexpr (META) {
+#pragma unroll
+            for (int j = 0; j < TILE_NPT; ++j) {
+                const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
+                const bool v = i < (unsigned)S.nfluid;
+                mr[j] = v ? __ldg(S.meta + i) : make_uint4(0, 0, 0, 0);
+                mr2[j] = v ? __ldg(S.meta2 + i) : make_uint2(0, 0);
+            }
+        }
+#pragma unroll
         for (int j = 0; j < TILE_NPT; ++j) {
             const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
             if (i >= (unsigned)S.nfluid) continue;
             CNb nb;
             if constexpr (META) {
-                meta_nbrs(S, i, nb);
+                meta_nbrs(S, i, mr[j], mr2[j], nb);
             } else {
                 int x, y, z;
                 coords3(S, __ldg(S.fnode + i), x, y, z);
@@ -516,6 +539,82 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
             }
             Cp ux, uy, uz;
             collide3<ST, W1>(g, S, ux, uy, uz);
+            ST::st(A + i, g[0]);
+#pragma unroll
+            for (int k = 1; k < Q3; ++k) {
+                const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
+                ST::st(A + dst, g[k]);
+            }
+            acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+        }
+        if (red) finish_tile(S, item.y, n, acc, sh);
+    }
+}
+
+// Even step with its gathers staged in shared memory by cp.async: the pulls
+// of all TILE_NPT voxels of a thread are issued (address from the neighbour
+// record, copy straight to shared memory, no register held) before the first
+// voxel is collided, so twice the loads are in flight per thread and the
+// register budget stays small enough for high occupancy.  Stores go straight
+// to global memory; their addresses are decoded again from the record.
+template <class ST, int MINB, bool W1>
+__global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    using Cp = typename ST::C;
+    using Wd = typename ST::W;
+    __shared__ double sh[TPB / 32][3];
+    __shared__ Wd stage[TILE_NPT][Q3][TPB];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S = a.solves[item.x];
+        const int phase = S.st->phase;
+        if (phase >= PH_DONE) continue;
+        const long long n = S.st->s_base + a.step + 1;
+        const bool red = needs_reduction(S.c, phase, n);
+        T *__restrict__ A = static_cast<T *>(S.A);
+        const unsigned P = (unsigned)S.plane;
+        double acc[3] = {0.0, 0.0, 0.0};
+        uint4 mr[TILE_NPT];
+        uint2 mr2[TILE_NPT];
+        unsigned par[TILE_NPT];          // bit k: parity of the pulled element (2-byte storage)
+#pragma unroll
+        for (int j = 0; j < TILE_NPT; ++j) {
+            const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
+            const bool v = i < (unsigned)S.nfluid;
+            mr[j] = v ? __ldg(S.meta + i) : make_uint4(0, 0, 0, 0);
+            mr2[j] = v ? __ldg(S.meta2 + i) : make_uint2(0, 0);
+        }
+#pragma unroll
+        for (int j = 0; j < TILE_NPT; ++j) {
+            const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
+            par[j] = 0;
+            if (i < (unsigned)S.nfluid) {
+                CNb nb;
+                meta_nbrs(S, i, mr[j], mr2[j], nb);
+#pragma unroll
+                for (int k = 0; k < Q3; ++k) {
+                    const int o = opp3(k);
+                    const unsigned src = k == 0 ? i : (((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]));
+                    par[j] |= (src & 1u) << k;
+                    __pipeline_memcpy_async(&stage[j][k][threadIdx.x], ST::word(A + src), sizeof(Wd));
+                }
+            }
+            __pipeline_commit();
+        }
+#pragma unroll
+        for (int j = 0; j < TILE_NPT; ++j) {
+            __pipeline_wait_prior(TILE_NPT - 1 - j);
+            const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
+            if (i >= (unsigned)S.nfluid) continue;
+            Cp g[Q3];
+#pragma unroll
+            for (int k = 0; k < Q3; ++k) g[k] = ST::unword(stage[j][k][threadIdx.x], (par[j] >> k) & 1u);
+            Cp ux, uy, uz;
+            collide3<ST, W1>(g, S, ux, uy, uz);
+            CNb nb;
+            meta_nbrs(S, i, mr[j], mr2[j], nb);
             ST::st(A + i, g[0]);
 #pragma unroll
             for (int k = 1; k < Q3; ++k) {

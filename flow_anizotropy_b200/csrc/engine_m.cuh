@@ -157,10 +157,14 @@ __global__ void __launch_bounds__(TPB, MINB) stepm_kernel(const StepArgs a)
                 // moments of the initial state f = w: rho = 1, j = 0
                 dr = C(0); ux = C(0.5) * Fx; uy = C(0.5) * Fy; uz = C(0.5) * Fz;
             } else {
-                int x, y, z;
-                coords3(S, __ldg(S.fnode + i), x, y, z);
                 CNb nb;
-                compact_nbrs(S, i, x, y, z, nb);
+                if (S.meta) {
+                    meta_nbrs(S, i, __ldg(S.meta + i), __ldg(S.meta2 + i), nb);
+                } else {
+                    int x, y, z;
+                    coords3(S, __ldg(S.fnode + i), x, y, z);
+                    compact_nbrs(S, i, x, y, z, nb);
+                }
                 C od, ox, oy, oz;
                 MT::ld(src, i, od, ox, oy, oz);
                 SrcM<C> own;

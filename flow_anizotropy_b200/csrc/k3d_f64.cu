@@ -23,7 +23,11 @@ cudaError_t launch_step3d_f64(int variant, bool odd, dim3 grid, cudaStream_t s, 
         case 0: LBM_EVEN(0)<<<grid, TPB, 0, s>>>(a); break;
         case 1: LBM_EVEN(1)<<<grid, TPB, 0, s>>>(a); break;
         case 2: LBM_EVEN(2)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_EVEN(3)<<<grid, TPB, 0, s>>>(a); break;
+        case 3: LBM_EVEN(3)<<<grid, TPB, 0, s>>>(a); break;
+        // FP64 staging would exceed the static shared-memory limit: variants
+        // 4-5 run the register-staged kernel with the same record reads
+        case 4: LBM_EVEN(0)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_EVEN(1)<<<grid, TPB, 0, s>>>(a); break;
         }
     }
     return cudaGetLastError();
@@ -34,7 +38,8 @@ int max_blocks_f64(int variant, bool odd)
     const int vo = variant / NVAR_EVEN, ve = variant % NVAR_EVEN;
     const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(0) : vo == 1 ? (const void *)LBM_ODD(1) : (const void *)LBM_ODD(2))
                         : (ve == 0 ? (const void *)LBM_EVEN(0) : ve == 1 ? (const void *)LBM_EVEN(1)
-                           : ve == 2 ? (const void *)LBM_EVEN(2) : (const void *)LBM_EVEN(3));
+                           : ve == 2 ? (const void *)LBM_EVEN(2) : ve == 3 ? (const void *)LBM_EVEN(3)
+                           : ve == 4 ? (const void *)LBM_EVEN(0) : (const void *)LBM_EVEN(1));
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;

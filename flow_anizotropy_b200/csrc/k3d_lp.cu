@@ -10,6 +10,7 @@ int max_blocks_f64(int variant, bool odd);
 
 #define LBM_ODD(ST, V, W) step3d_odd_kernel<ST, odd_lp(V).npt, odd_lp(V).minb, W>
 #define LBM_EVEN(ST, V, W) step3d_even_kernel<ST, even_lp(V).minb, W, even_meta(V)>
+#define LBM_EVENA(ST, V, W) step3d_even_async_kernel<ST, even_lp(V).minb, W>
 
 template <class ST, bool W>
 static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
@@ -27,7 +28,9 @@ static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const S
         case 0: LBM_EVEN(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
         case 1: LBM_EVEN(ST, 1, W)<<<grid, TPB, 0, s>>>(a); break;
         case 2: LBM_EVEN(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_EVEN(ST, 3, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 3: LBM_EVEN(ST, 3, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 4: LBM_EVENA(ST, 4, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_EVENA(ST, 5, W)<<<grid, TPB, 0, s>>>(a); break;
         }
     }
     return cudaGetLastError();
@@ -50,7 +53,8 @@ static int occ(int v, bool odd)
     const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(ST, 0, true) : vo == 1 ? (const void *)LBM_ODD(ST, 1, true)
                                                                         : (const void *)LBM_ODD(ST, 2, true))
                         : (ve == 0 ? (const void *)LBM_EVEN(ST, 0, true) : ve == 1 ? (const void *)LBM_EVEN(ST, 1, true)
-                           : ve == 2 ? (const void *)LBM_EVEN(ST, 2, true) : (const void *)LBM_EVEN(ST, 3, true));
+                           : ve == 2 ? (const void *)LBM_EVEN(ST, 2, true) : ve == 3 ? (const void *)LBM_EVEN(ST, 3, true)
+                           : ve == 4 ? (const void *)LBM_EVENA(ST, 4, true) : (const void *)LBM_EVENA(ST, 5, true));
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;
