@@ -9,12 +9,16 @@ porosity 0.45, percolating in x, y and z (seeded, synthetic), solved along
 three directions run concurrently on one GPU.
 
 Reported (one JSON line, rank 0):
-  value      k-tensors/hour of the headline path (default: FP16 shifted
-             storage, FP32 collision, FP64 reductions), inputs resident in HBM,
-             device time from CUDA events on the solver's stream;
+  value      k-tensors/hour of the headline path, the fastest of FP32
+             populations, FP16 populations and the tau = 1 FP32 moment form that
+             stays within 1e-3 of the FP64 tensor (every path keeps the
+             reference's stopping rule), inputs resident in HBM, device time
+             from CUDA events on the solver's stream;
   e2e        the same through the public API with the structure in host memory
              (host->device copy and result read-back inside the timed region);
   plain_fp32 the same workload with plain FP32 storage, one launch per step;
+  serving    p50/p99 latency of a short 20 requests/s Poisson trace through the
+             continuous-batching server;
   rel_err    the headline K against the FP64 K of the same structure;
   roofline   HBM roofline of the step kernel: algorithmic bytes (pore voxels
              x 2 x 19 x element size + N/8 mask) / time, against the measured
@@ -55,7 +59,12 @@ METRIC = "k-tensors/hr & GLUPS at ≤1e-3 rel err vs FP64, vs plain FP32; p50/p9
 WORKLOAD = dict(workload="perm-tensor 128^3 prolate-ellipsoid packing (4,4,12) phi=0.45, 3 directions",
                 n=128, semi=(4.0, 4.0, 12.0), porosity=0.45, seed=0, ff=4.0, tau=1.0, eps=1e-6,
                 lag=1000, hold=2, min_steps=4000, max_steps=50000, avg_steps=2000)
-BYTES_PER_UPDATE = {"fp64": 304, "fp32": 152, "fp16": 76, "bf16": 76}
+# algorithmic bytes per pore-voxel update: populations read + written once
+# (AA pattern), or for the tau = 1 moment form a 20-byte record read + written
+BYTES_PER_UPDATE = {"fp64": 304, "fp32": 152, "fp16": 76, "bf16": 76, "m32": 40, "m64": 80}
+DTYPE = {"fp16": "f16-storage/f32-compute/f64-reduce", "bf16": "bf16-storage/f32-compute/f64-reduce",
+         "fp32": "f32-storage/f32-compute/f64-reduce", "fp64": "f64",
+         "m32": "f32 moment records (tau=1)/f32-compute/f64-reduce", "m64": "f64 moment records (tau=1)"}
 # Steps per direction of the converged FP64 solve of the workload structure
 # (x, y, z).  Our FP64 path reproduces the reference's step counts exactly
 # (per-step bit-identical populations; see tests/test_gpu_solve3d.py); the
@@ -224,6 +233,33 @@ def cpu_baseline_entry(cpu, N, steps64):
             f"{list(map(int, steps64))}", "mlups_per_core": cpu["lups_per_core"] / 1e6}
 
 
+# ---------------------------------------------------------------- serving ----
+def serve_trace(device, prec, args):
+    """Short Poisson trace at the serving rate (20 requests/s) through the
+    continuous-batching server: structures of the uneven-size mix restricted
+    to its two smallest edges (48, 64) so the trace drains in seconds."""
+    from flow_anizotropy_b200 import structures as st
+    from flow_anizotropy_b200.serve import Server, poisson_arrivals, replay
+    from flow_anizotropy_b200.solver import Params3D
+    mix = [d for d in st.batch_mix(64, seed=5) if d["n"] in (48, 64)][:8]
+    pool = [st.make(d) for d in mix]
+    F = 2.5e-7 * WORKLOAD["ff"]
+    p = Params3D(tau=1.0, eps=WORKLOAD["eps"], lag=WORKLOAD["lag"], hold=WORKLOAD["hold"],
+                 min_steps=WORKLOAD["min_steps"], max_steps=WORKLOAD["max_steps"],
+                 avg_steps=WORKLOAD["avg_steps"], precision=prec)
+    forces = [[F, 0, 0], [0, F, 0], [0, 0, F]]
+    srv = Server(precision=prec, hbm_budget=150 * 2**30, chunk=128, device=device)
+    arrivals = poisson_arrivals(20.0, args.serve_seconds, seed=11)
+    t0 = time.perf_counter()
+    stats = replay(srv, arrivals, lambda i: (pool[i % len(pool)], forces, p))
+    wall = time.perf_counter() - t0
+    srv.close()
+    return {"rate_per_s": 20.0, "arrival_seconds": args.serve_seconds, "requests": stats.completed,
+            "p50_s": stats.pct(50), "p99_s": stats.pct(99), "max_resident": stats.max_resident,
+            "k_tensors_per_hr": 3600.0 * stats.completed / wall,
+            "mix": "batch mix, edges 48 and 64 only (8 seeded structures, reused)", "path": prec}
+
+
 # -------------------------------------------------------------- our arm ----
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -284,69 +320,141 @@ def run_ours(args, rank, world, local_rank):
         return dict(prec=prec, variant=best, tune_ms=ms, ms=ms_total, runs=runs_all[-1], clocks=clk.summary(),
                     dir_steps=dir_steps, launches=launches)
 
-    head = measure(args.precision, args.warmup, args.steps)
-    plain = measure("fp32", max(1, min(args.warmup, 2)), max(1, min(args.steps, 3)))
-    e2e = measure(args.precision, 1, args.steps, host_input=True)
+    results = {}
+    cands = [args.precision] if args.precision != "auto" else ["fp32", "fp16", "m32"]
+    if "fp32" not in cands:
+        cands.append("fp32")
+    for prec in cands:
+        m = measure(prec, args.warmup, args.steps)
+        m["K"] = tensor_K(m["runs"], mu, F)
+        m["err"] = k_errors(m["K"], K64)
+        results[prec] = m
 
     def rates(m):
         sec = m["ms"] / 1e3
-        tensors = world * (args.steps if m is not plain else max(1, min(args.steps, 3)))
-        kt_hr = 3600.0 * tensors / sec
-        glups_fluid = world * m["dir_steps"] * npore / sec / 1e9
-        glups_all = world * m["dir_steps"] * N / sec / 1e9
-        return kt_hr, glups_fluid, glups_all
+        tensors = world * args.steps
+        return (3600.0 * tensors / sec, world * m["dir_steps"] * npore / sec / 1e9,
+                world * m["dir_steps"] * N / sec / 1e9)
 
+    ok = [p_ for p_ in results if results[p_]["err"]["max_rel"] <= 1e-3]
+    head_prec = max(ok, key=lambda p_: rates(results[p_])[0]) if ok else "fp32"
+    head = results[head_prec]
+    plain = results["fp32"]
+    e2e = measure(head_prec, 1, args.steps, host_input=True)
     kt, gf, ga = rates(head)
     kt_p, gf_p, ga_p = rates(plain)
     kt_e, _, _ = rates(e2e)
-    Kh = tensor_K(head["runs"], mu, F)
-    Kp = tensor_K(plain["runs"], mu, F)
     peak, peak_kind = measured_peak()
-    B = BYTES_PER_UPDATE[args.precision]
+    B = BYTES_PER_UPDATE[head_prec]
     alg_bytes = head["dir_steps"] * (npore * B + N / 8.0)
     achieved = alg_bytes / (head["ms"] / 1e3) / 1e9
     per_launch_alg = alg_bytes / max(1, head["launches"])
     traffic = profiled_traffic()
+    serving = serve_trace(device, head_prec, args) if args.serve_seconds > 0 else None
     out = None
     if rank == 0:
         cpu = cpu_sample(solid, wl, seconds_target=args.cpu_seconds)
         cpu_entry = cpu_baseline_entry(cpu, N, steps64)
+        paths = {}
+        for p_, m in results.items():
+            k_, g_, a_ = rates(m)
+            paths[p_] = {"k_tensors_per_hr": k_, "glups_fluid": g_, "glups_all_node": a_,
+                         "steps_per_direction": [r.steps for r in m["runs"]],
+                         "converged": [r.converged for r in m["runs"]],
+                         "rel_err_vs_fp64": m["err"], "kernel_variant": m["variant"],
+                         "hbm_gbs_alg": m["dir_steps"] * (npore * BYTES_PER_UPDATE[p_] + N / 8.0) / (m["ms"] / 1e3) / 1e9}
         out = {
             "metric": METRIC, "value": kt, "unit": "k-tensors/hr", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": {"fp16": "f16-storage/f32-compute/f64-reduce",
-                                                              "bf16": "bf16-storage/f32-compute/f64-reduce",
-                                                              "fp32": "f32", "fp64": "f64"}[args.precision],
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[head_prec],
             "data": "synthetic (seeded structure; no dataset)",
             "config": {"workload": wl["workload"], "seed": wl["seed"], "tau": wl["tau"], "g": F,
-                       "eps": wl["eps"], "lag": wl["lag"], "max_steps": wl["max_steps"],
-                       "precision": args.precision, "kernel_variant": head["variant"],
-                       "criterion": "block-mean k-sigma" if args.precision in ("fp16", "bf16") else "drift (reference)",
+                       "eps": wl["eps"], "lag": wl["lag"], "hold": wl["hold"], "min_steps": wl["min_steps"],
+                       "max_steps": wl["max_steps"], "avg_steps": wl["avg_steps"],
+                       "path": head_prec, "kernel_variant": head["variant"],
+                       "criterion": "block-mean k-sigma" if head_prec in ("fp16", "bf16") else "drift (reference)",
                        "parallelism": f"work partition x{world} (one tensor stream per GPU)",
-                       "l2": "lattice (3 x 19 x pores x elem) exceeds L2 only for fp32/fp64; each tensor is a "
-                             "fresh solve streaming its lattice every step"},
+                       "l2": "lattices (3 x 19 x 0.94 M pores x elem: 215 MB fp32, 108 MB fp16) stream from HBM "
+                             "every step; inputs are the whole tensor solve, not a cached kernel"},
             "glups_fluid": gf, "glups_all_node": ga,
             "steps_per_direction": [r.steps for r in head["runs"]],
-            "converged": [r.converged for r in head["runs"]],
-            "rel_err_vs_fp64": k_errors(Kh, K64),
-            "plain_fp32": {"value": kt_p, "unit": "k-tensors/hr", "glups_fluid": gf_p, "glups_all_node": ga_p,
-                           "steps_per_direction": [r.steps for r in plain["runs"]],
-                           "rel_err_vs_fp64": k_errors(Kp, K64), "kernel_variant": plain["variant"]},
+            "rel_err_vs_fp64": head["err"],
+            "paths": paths,
+            "plain_fp32": {"value": kt_p, "unit": "k-tensors/hr", "glups_fluid": gf_p, "glups_all_node": ga_p},
             "speedup_vs_plain_fp32": kt / kt_p,
             "fp64_steps_per_direction": steps64,
+            "serving": serving,
             "e2e": {"value": kt_e, "unit": "k-tensors/hr", "h2d_bytes_per_step": int(N),
                     "d2h_bytes_per_step": int(3 * 64)},
             "gpu_launches": int(head["launches"] + 8 * args.steps),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "alg_bytes_per_launch": per_launch_alg,
-                         "kernel": f"step3d_kernel<{args.precision}, variant {head['variant']}>"},
+                         "kernel": f"step3d ({head_prec}) variant {head['variant']}"},
             "cpu_baseline": cpu_entry,
             "clocks": head["clocks"],
         }
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return out
+
+
+# ------------------------------------------------------- batched workload --
+def _make_structure(d):
+    from flow_anizotropy_b200 import structures as st
+    return st.make(d)
+
+
+def run_batch_workload(args, device=0):
+    """The uneven-size mix: `count` structures with edges from {48,64,96,128,160},
+    three directions each, solved (a) one structure at a time with plain FP32
+    per-step launches, (b) all resident in one batch (CUDA-graph chunks,
+    per-solve retirement) for each batched path.  Reports k-tensors/hour."""
+    import multiprocessing as mproc
+    import torch
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200 import solver as S
+    from flow_anizotropy_b200 import structures as st
+    mix = st.batch_mix(args.count, seed=0)
+    with mproc.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        structs = pool.map(_make_structure, mix)
+    F = 2.5e-7 * WORKLOAD["ff"]
+    forces = [[F, 0, 0], [0, F, 0], [0, 0, F]]
+    ctx = _lib.context(device)
+
+    def params(prec):
+        return S.Params3D(tau=1.0, eps=WORKLOAD["eps"], lag=WORKLOAD["lag"], hold=WORKLOAD["hold"],
+                          min_steps=WORKLOAD["min_steps"], max_steps=WORKLOAD["max_steps"],
+                          avg_steps=WORKLOAD["avg_steps"], precision=prec)
+
+    out = {"workload": f"batch mix of {args.count} structures (edges 48..160, 3 directions)",
+           "voxels": int(sum(s.size for s in structs)), "pores": int(sum((s == 0).sum() for s in structs))}
+    ref = {}
+    with EventTimer(torch, ctx.stream) as t:
+        for i, s_ in enumerate(structs):
+            runs, _, _ = S.solve3d(s_, forces, params("fp32"), device=device)
+            ref[i] = runs
+    out["plain_fp32_per_solve"] = {"seconds": t.ms / 1e3, "k_tensors_per_hr": 3600 * len(structs) / (t.ms / 1e3)}
+    for prec in args.batch_paths.split(","):
+        b = S.Batch(precision=prec, hbm_budget=150 * 2**30, chunk=256, device=device)
+        done = {}
+        with EventTimer(torch, ctx.stream) as t:
+            for i, s_ in enumerate(structs):
+                assert b.submit(s_, forces, params(prec), tag=i)
+            while len(done) < len(structs):
+                b.run(4)
+                done.update(dict(b.poll()))
+        b.close()
+        worst = 0.0
+        for i in done:
+            for a_, m_ in zip(ref[i], done[i]):
+                sc = np.abs(a_.q).max()
+                worst = max(worst, float(np.abs(a_.q - m_.q).max() / sc))
+        out[f"batched_{prec}"] = {"seconds": t.ms / 1e3, "k_tensors_per_hr": 3600 * len(structs) / (t.ms / 1e3),
+                                  "max_rel_q_vs_plain_fp32": worst}
+    out["speedup_vs_plain_fp32"] = {k: out["plain_fp32_per_solve"]["seconds"] / v["seconds"]
+                                    for k, v in out.items() if k.startswith("batched_")}
     return out
 
 
@@ -384,7 +492,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16", "fp32", "fp64"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32"])
+    ap.add_argument("--serve-seconds", type=float, default=5.0)
+    ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch"])
+    ap.add_argument("--count", type=int, default=32, help="structures of the batch workload")
+    ap.add_argument("--batch-paths", default="fp32,m32,fp16")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -392,6 +504,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "batch":
+        out = run_batch_workload(args, local_rank) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None and rank == 0:

@@ -166,14 +166,14 @@ long long lbm_plane_elems(long long nn) { return (nn + 63) / 64 * 64; }
 // Lattice bytes of one direction over n pore voxels.
 long long lbm_lattice_bytes3d(long long n, int prec)
 {
-    if (is_moment(prec)) return 2ll * 16ll * mom_buffer_elems(prec, n);
+    if (is_moment(prec)) return 2ll * mom_buffer_bytes(prec, n);
     return (long long)Q3 * lbm_plane_elems(n) * (long long)elem_size(prec);
 }
 
-// Plane stride (populations) or buffer length in 16-byte elements (moments).
+// Plane stride (populations) or record slots per buffer (moments).
 long long lbm_plane_for(int prec, long long n)
 {
-    return is_moment(prec) ? mom_buffer_elems(prec, n) : lbm_plane_elems(n);
+    return is_moment(prec) ? mom_slots(n) : lbm_plane_elems(n);
 }
 
 // A variant whose even kernel reads neighbour records needs them built.

@@ -17,94 +17,103 @@
 
 namespace lbm {
 
+// State per pore voxel, written by the voxel's own update and read by its
+// up to 19 receivers: (c1, d3, ux, uy, uz) with
+//   c1 = drho - 1.5 rho u^2 - 3 pr u.F   (the direction-independent part),
+//   d3 = 3 drho                          (3 rho - 3, kept shifted for precision),
+// so a receiver evaluates a post-collision population without recomputing
+// per-source invariants:
+//   f*_k - w_k = w_k [c1 + eu (r3 + 1.5 r3 eu) + pr eF_k (3 + 9 eu)],
+//   r3 = 3 + d3, eu = e_k . u, eF_k = e_k . F.
+// A buffer holds `slots` records: a float4/double2x2 part (c1, ux, uy, uz)
+// followed by the d3 part.
 struct MomF32 {
-    using T = float4;
     using C = float;
     static constexpr int code = 4;
-    __device__ static __forceinline__ void ld(const T *b, unsigned i, C &d, C &x, C &y, C &z)
+    static constexpr size_t rec_bytes = 20;
+    __device__ static __forceinline__ void ld(const void *buf, long long slots, unsigned i, C &c1, C &d3, C &x, C &y, C &z)
     {
-        const float4 v = __ldg(b + i);
-        d = v.x; x = v.y; y = v.z; z = v.w;
+        const float4 v = __ldg(static_cast<const float4 *>(buf) + i);
+        c1 = v.x; x = v.y; y = v.z; z = v.w;
+        d3 = __ldg(reinterpret_cast<const float *>(static_cast<const float4 *>(buf) + slots) + i);
     }
-    __device__ static __forceinline__ void st(T *b, unsigned i, C d, C x, C y, C z)
+    __device__ static __forceinline__ void st(void *buf, long long slots, unsigned i, C c1, C d3, C x, C y, C z)
     {
-        b[i] = make_float4(d, x, y, z);
+        static_cast<float4 *>(buf)[i] = make_float4(c1, x, y, z);
+        reinterpret_cast<float *>(static_cast<float4 *>(buf) + slots)[i] = d3;
     }
 };
 
 struct MomF64 {
-    using T = double2;       // two double2 per voxel: (drho, ux), (uy, uz)
     using C = double;
     static constexpr int code = 5;
-    __device__ static __forceinline__ void ld(const T *b, unsigned i, C &d, C &x, C &y, C &z)
+    static constexpr size_t rec_bytes = 40;
+    __device__ static __forceinline__ void ld(const void *buf, long long slots, unsigned i, C &c1, C &d3, C &x, C &y, C &z)
     {
+        const double2 *b = static_cast<const double2 *>(buf);
         const double2 a = __ldg(b + 2 * (size_t)i), c = __ldg(b + 2 * (size_t)i + 1);
-        d = a.x; x = a.y; y = c.x; z = c.y;
+        c1 = a.x; x = a.y; y = c.x; z = c.y;
+        d3 = __ldg(reinterpret_cast<const double *>(b + 2 * slots) + i);
     }
-    __device__ static __forceinline__ void st(T *b, unsigned i, C d, C x, C y, C z)
+    __device__ static __forceinline__ void st(void *buf, long long slots, unsigned i, C c1, C d3, C x, C y, C z)
     {
-        b[2 * (size_t)i] = make_double2(d, x);
+        double2 *b = static_cast<double2 *>(buf);
+        b[2 * (size_t)i] = make_double2(c1, x);
         b[2 * (size_t)i + 1] = make_double2(y, z);
+        reinterpret_cast<double *>(b + 2 * slots)[i] = d3;
     }
 };
 
-// Elements of T per buffer (padded to 128 B); the two buffers are contiguous.
-inline long long mom_buffer_elems(int prec, long long nfluid)
+// Record slots per buffer (padded so both parts stay 128-byte aligned).
+inline long long mom_slots(long long nfluid) { return (nfluid + 31) / 32 * 32; }
+inline long long mom_buffer_bytes(int prec, long long nfluid)
 {
-    const long long per = prec == MomF32::code ? 1 : 2;
-    return (nfluid * per + 7) / 8 * 8;
+    return mom_slots(nfluid) * (prec == MomF32::code ? (long long)MomF32::rec_bytes : (long long)MomF64::rec_bytes);
 }
 
-// Post-collision shifted population k (f*_k - w_k) of a voxel with moments
-// (dr, u): w_k [c1 + eu (3 rho + 4.5 rho eu) + pr eF_k (3 + 9 eu)], with
-// c1 = dr - 1.5 rho u^2 - 3 pr u.F.  Accumulated straight into the moments of
-// the receiving voxel.
+// The record of a voxel with moments (drho, u).
 template <class C>
-struct SrcM {
-    C c1, r3, r45, ux, uy, uz;
-    __device__ __forceinline__ void set(C dr, C x, C y, C z, C Fx, C Fy, C Fz, C pr)
-    {
-        const C rho = C(1) + dr;
-        const C u2 = x * x + y * y + z * z;
-        const C uF = x * Fx + y * Fy + z * Fz;
-        c1 = dr - C(1.5) * rho * u2 - C(3) * pr * uF;
-        r3 = C(3) * rho;
-        r45 = C(4.5) * rho;
-        ux = x; uy = y; uz = z;
-    }
-};
+__device__ __forceinline__ void make_record(C dr, C x, C y, C z, C Fx, C Fy, C Fz, C pr, C &c1, C &d3)
+{
+    const C rho = C(1) + dr;
+    const C u2 = x * x + y * y + z * z;
+    const C uF = x * Fx + y * Fy + z * Fz;
+    c1 = dr - C(1.5) * rho * u2 - C(3) * pr * uF;
+    d3 = C(3) * dr;
+}
 
+// f*_k - w_k of a source with record (c1, d3, u); sgn = -1 evaluates the
+// opposite direction (bounce-back: f*_opp(k) of the receiving voxel itself).
 template <int K, class C>
-__device__ __forceinline__ C pop_from(const SrcM<C> &s, C pr, C Fx, C Fy, C Fz)
+__device__ __forceinline__ C pop_rec(C c1, C d3, C ux, C uy, C uz, C sgn, C pr, C Fx, C Fy, C Fz)
 {
     constexpr int cx = ex3(K), cy = ey3(K), cz = ez3(K);
     C eu = C(0), eF = C(0);
-    if (cx) { eu += cx > 0 ? s.ux : -s.ux; eF += cx > 0 ? Fx : -Fx; }
-    if (cy) { eu += cy > 0 ? s.uy : -s.uy; eF += cy > 0 ? Fy : -Fy; }
-    if (cz) { eu += cz > 0 ? s.uz : -s.uz; eF += cz > 0 ? Fz : -Fz; }
+    if (cx) { eu += cx > 0 ? ux : -ux; eF += cx > 0 ? Fx : -Fx; }
+    if (cy) { eu += cy > 0 ? uy : -uy; eF += cy > 0 ? Fy : -Fy; }
+    if (cz) { eu += cz > 0 ? uz : -uz; eF += cz > 0 ? Fz : -Fz; }
     const C w = (C)w3(K);
-    if constexpr (K == 0) return w * s.c1;
-    return w * (s.c1 + eu * (s.r3 + s.r45 * eu) + pr * eF * (C(3) + C(9) * eu));
+    if constexpr (K == 0) return w * c1;
+    eu *= sgn;
+    eF *= sgn;
+    const C r3 = C(3) + d3;
+    return w * (c1 + eu * (r3 + C(1.5) * r3 * eu) + pr * eF * (C(3) + C(9) * eu));
 }
 
 template <int K, class MT>
-__device__ __forceinline__ void gather_one(const typename MT::T *__restrict__ src, unsigned i, const CNb &nb,
-                                           const SrcM<typename MT::C> &own, typename MT::C pr,
-                                           typename MT::C Fx, typename MT::C Fy, typename MT::C Fz,
-                                           typename MT::C (&acc)[4])
+__device__ __forceinline__ void gather_rec(const void *src, long long slots, unsigned i, const CNb &nb,
+                                           typename MT::C pr, typename MT::C Fx, typename MT::C Fy,
+                                           typename MT::C Fz, typename MT::C (&acc)[4])
 {
     using C = typename MT::C;
     constexpr int o = opp3(K);
-    C g;
-    if ((nb.solid >> o) & 1u) {
-        g = pop_from<o, C>(own, pr, Fx, Fy, Fz);      // bounce back: f*_opp(k)(x)
-    } else {
-        C d, x, y, z;
-        MT::ld(src, nb.idx[o], d, x, y, z);
-        SrcM<C> s;
-        s.set(d, x, y, z, Fx, Fy, Fz, pr);
-        g = pop_from<K, C>(s, pr, Fx, Fy, Fz);        // pull f*_k(x - e_k)
-    }
+    // pull f*_k(x - e_k), or across a solid link f*_opp(k)(x): the same
+    // formula on the voxel's own record with the direction reversed
+    const bool bb = (nb.solid >> o) & 1u;
+    const unsigned from = bb ? i : nb.idx[o];
+    C c1, d3, x, y, z;
+    MT::ld(src, slots, from, c1, d3, x, y, z);
+    const C g = pop_rec<K, C>(c1, d3, x, y, z, bb ? C(-1) : C(1), pr, Fx, Fy, Fz);
     acc[0] += g;
     if (ex3(K)) acc[1] += ex3(K) > 0 ? g : -g;
     if (ey3(K)) acc[2] += ey3(K) > 0 ? g : -g;
@@ -112,27 +121,24 @@ __device__ __forceinline__ void gather_one(const typename MT::T *__restrict__ sr
 }
 
 template <class MT, int K>
-struct GatherAll {
-    __device__ __forceinline__ static void run(const typename MT::T *src, unsigned i, const CNb &nb,
-                                               const SrcM<typename MT::C> &own, typename MT::C pr,
-                                               typename MT::C Fx, typename MT::C Fy, typename MT::C Fz,
-                                               typename MT::C (&acc)[4])
+struct GatherRec {
+    __device__ __forceinline__ static void run(const void *src, long long slots, unsigned i, const CNb &nb,
+                                               typename MT::C pr, typename MT::C Fx, typename MT::C Fy,
+                                               typename MT::C Fz, typename MT::C (&acc)[4])
     {
-        gather_one<K, MT>(src, i, nb, own, pr, Fx, Fy, Fz, acc);
-        GatherAll<MT, K + 1>::run(src, i, nb, own, pr, Fx, Fy, Fz, acc);
+        gather_rec<K, MT>(src, slots, i, nb, pr, Fx, Fy, Fz, acc);
+        GatherRec<MT, K + 1>::run(src, slots, i, nb, pr, Fx, Fy, Fz, acc);
     }
 };
 template <class MT>
-struct GatherAll<MT, Q3> {
-    __device__ __forceinline__ static void run(const typename MT::T *, unsigned, const CNb &,
-                                               const SrcM<typename MT::C> &, typename MT::C, typename MT::C,
-                                               typename MT::C, typename MT::C, typename MT::C (&)[4]) {}
+struct GatherRec<MT, Q3> {
+    __device__ __forceinline__ static void run(const void *, long long, unsigned, const CNb &, typename MT::C,
+                                               typename MT::C, typename MT::C, typename MT::C, typename MT::C (&)[4]) {}
 };
 
 template <class MT, int MINB>
 __global__ void __launch_bounds__(TPB, MINB) stepm_kernel(const StepArgs a)
 {
-    using T = typename MT::T;
     using C = typename MT::C;
     __shared__ double sh[TPB / 32][3];
     const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
@@ -143,10 +149,11 @@ __global__ void __launch_bounds__(TPB, MINB) stepm_kernel(const StepArgs a)
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
         const bool red = needs_reduction(S.c, phase, n);
-        T *base = static_cast<T *>(S.A);
-        const long long per = S.plane;                 // elements of T per buffer
-        T *dst = base + (n & 1ll) * per;
-        const T *src = base + ((n + 1) & 1ll) * per;
+        char *base = static_cast<char *>(S.A);
+        const long long slots = S.plane;
+        const long long bytes = slots * (long long)MT::rec_bytes;
+        void *dst = base + (n & 1ll) * bytes;
+        const void *src = base + ((n + 1) & 1ll) * bytes;
         const C Fx = (C)S.P.F[0], Fy = (C)S.P.F[1], Fz = (C)S.P.F[2];
         const C pr = (C)S.P.pref;
         double acc3[3] = {0.0, 0.0, 0.0};
@@ -165,75 +172,63 @@ __global__ void __launch_bounds__(TPB, MINB) stepm_kernel(const StepArgs a)
                     coords3(S, __ldg(S.fnode + i), x, y, z);
                     compact_nbrs(S, i, x, y, z, nb);
                 }
-                C od, ox, oy, oz;
-                MT::ld(src, i, od, ox, oy, oz);
-                SrcM<C> own;
-                own.set(od, ox, oy, oz, Fx, Fy, Fz, pr);
-                C acc[4] = {C(0), C(0), C(0), C(0)};
-                acc[0] = pop_from<0, C>(own, pr, Fx, Fy, Fz);
-                GatherAll<MT, 1>::run(src, i, nb, own, pr, Fx, Fy, Fz, acc);
+                C c1, d3, ox, oy, oz;
+                MT::ld(src, slots, i, c1, d3, ox, oy, oz);
+                C acc[4] = {pop_rec<0, C>(c1, d3, ox, oy, oz, C(1), pr, Fx, Fy, Fz), C(0), C(0), C(0)};
+                GatherRec<MT, 1>::run(src, slots, i, nb, pr, Fx, Fy, Fz, acc);
                 dr = acc[0];
                 const C rho = C(1) + dr;
                 ux = (acc[1] + C(0.5) * Fx) / rho;
                 uy = (acc[2] + C(0.5) * Fy) / rho;
                 uz = (acc[3] + C(0.5) * Fz) / rho;
             }
-            MT::st(dst, i, dr, ux, uy, uz);
+            C c1n, d3n;
+            make_record<C>(dr, ux, uy, uz, Fx, Fy, Fz, pr, c1n, d3n);
+            MT::st(dst, slots, i, c1n, d3n, ux, uy, uz);
             acc3[0] = (double)ux; acc3[1] = (double)uy; acc3[2] = (double)uz;
         }
         if (red) finish_tile(S, item.y, n, acc3, sh);
     }
 }
 
-// Dense outputs from the moments of step `done`: velocity (the reference's U,
+// Dense outputs from the records of step `done`: velocity (the reference's U,
 // V, W) and/or the canonical post-collision populations f*_k = w_k + h_k.
 template <class MT>
 __global__ void canonm_kernel(const Solve3 S, long long done, double *f_out, float *u_out)
 {
-    using T = typename MT::T;
     using C = typename MT::C;
-    const T *base = static_cast<const T *>(S.A);
-    const T *cur = base + (done & 1ll) * S.plane;
+    const char *base = static_cast<const char *>(S.A);
+    const long long slots = S.plane;
+    const void *cur = base + (done & 1ll) * slots * (long long)MT::rec_bytes;
     const C Fx = (C)S.P.F[0], Fy = (C)S.P.F[1], Fz = (C)S.P.F[2];
     const C pr = (C)S.P.pref;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < (unsigned)S.nfluid;
          i += gridDim.x * blockDim.x) {
         const unsigned node = S.fnode[i];
-        C d, x, y, z;
-        if (done == 0) { d = C(0); x = C(0); y = C(0); z = C(0); }
-        else MT::ld(cur, i, d, x, y, z);
+        if (done == 0) {
+            if (u_out) {
+                u_out[3 * (size_t)node] = (float)(C(0.5) * Fx);
+                u_out[3 * (size_t)node + 1] = (float)(C(0.5) * Fy);
+                u_out[3 * (size_t)node + 2] = (float)(C(0.5) * Fz);
+            }
+            if (f_out)
+                for (int k = 0; k < Q3; ++k) f_out[(size_t)node * Q3 + k] = w3(k);
+            continue;
+        }
+        C c1, d3, x, y, z;
+        MT::ld(cur, slots, i, c1, d3, x, y, z);
         if (u_out) {
-            u_out[3 * (size_t)node] = (float)(done == 0 ? C(0.5) * Fx : x);
-            u_out[3 * (size_t)node + 1] = (float)(done == 0 ? C(0.5) * Fy : y);
-            u_out[3 * (size_t)node + 2] = (float)(done == 0 ? C(0.5) * Fz : z);
+            u_out[3 * (size_t)node] = (float)x;
+            u_out[3 * (size_t)node + 1] = (float)y;
+            u_out[3 * (size_t)node + 2] = (float)z;
         }
         if (f_out) {
-            if (done == 0) {
-                for (int k = 0; k < Q3; ++k) f_out[(size_t)node * Q3 + k] = w3(k);
-                continue;
-            }
-            SrcM<C> s;
-            s.set(d, x, y, z, Fx, Fy, Fz, pr);
             double f[Q3];
-            f[0] = w3(0) + (double)pop_from<0, C>(s, pr, Fx, Fy, Fz);
-            f[1] = w3(1) + (double)pop_from<1, C>(s, pr, Fx, Fy, Fz);
-            f[2] = w3(2) + (double)pop_from<2, C>(s, pr, Fx, Fy, Fz);
-            f[3] = w3(3) + (double)pop_from<3, C>(s, pr, Fx, Fy, Fz);
-            f[4] = w3(4) + (double)pop_from<4, C>(s, pr, Fx, Fy, Fz);
-            f[5] = w3(5) + (double)pop_from<5, C>(s, pr, Fx, Fy, Fz);
-            f[6] = w3(6) + (double)pop_from<6, C>(s, pr, Fx, Fy, Fz);
-            f[7] = w3(7) + (double)pop_from<7, C>(s, pr, Fx, Fy, Fz);
-            f[8] = w3(8) + (double)pop_from<8, C>(s, pr, Fx, Fy, Fz);
-            f[9] = w3(9) + (double)pop_from<9, C>(s, pr, Fx, Fy, Fz);
-            f[10] = w3(10) + (double)pop_from<10, C>(s, pr, Fx, Fy, Fz);
-            f[11] = w3(11) + (double)pop_from<11, C>(s, pr, Fx, Fy, Fz);
-            f[12] = w3(12) + (double)pop_from<12, C>(s, pr, Fx, Fy, Fz);
-            f[13] = w3(13) + (double)pop_from<13, C>(s, pr, Fx, Fy, Fz);
-            f[14] = w3(14) + (double)pop_from<14, C>(s, pr, Fx, Fy, Fz);
-            f[15] = w3(15) + (double)pop_from<15, C>(s, pr, Fx, Fy, Fz);
-            f[16] = w3(16) + (double)pop_from<16, C>(s, pr, Fx, Fy, Fz);
-            f[17] = w3(17) + (double)pop_from<17, C>(s, pr, Fx, Fy, Fz);
-            f[18] = w3(18) + (double)pop_from<18, C>(s, pr, Fx, Fy, Fz);
+#define LBM_POP(K) f[K] = w3(K) + (double)pop_rec<K, C>(c1, d3, x, y, z, C(1), pr, Fx, Fy, Fz);
+            LBM_POP(0) LBM_POP(1) LBM_POP(2) LBM_POP(3) LBM_POP(4) LBM_POP(5) LBM_POP(6) LBM_POP(7) LBM_POP(8)
+            LBM_POP(9) LBM_POP(10) LBM_POP(11) LBM_POP(12) LBM_POP(13) LBM_POP(14) LBM_POP(15) LBM_POP(16)
+            LBM_POP(17) LBM_POP(18)
+#undef LBM_POP
             for (int k = 0; k < Q3; ++k) f_out[(size_t)node * Q3 + k] = f[k];
         }
     }

@@ -138,3 +138,11 @@ def test_capi_exports_every_declared_symbol():
         assert hasattr(L, n), n
     assert set(names) == set(_lib.SYMBOLS)
     assert L.lbm_version() == 1
+
+
+def test_poisson_arrivals():
+    from flow_anizotropy_b200.serve import poisson_arrivals
+    a = poisson_arrivals(20.0, 100.0, seed=1)
+    assert a == poisson_arrivals(20.0, 100.0, seed=1)
+    assert all(x < y for x, y in zip(a, a[1:])) and a[-1] < 100.0
+    assert 1800 < len(a) < 2200
