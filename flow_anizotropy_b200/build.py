@@ -31,6 +31,7 @@ UNITS = {
     "k3d_m.cu": [],
     "engine.cu": [],
     "engine2.cu": [],
+    "engine2_noalloc.cu": [],
     "engine_batch.cu": [],
 }
 

@@ -11,11 +11,12 @@
 
 #include "../../include/lbm.h"
 #include "engine2d.cuh"
+#include "engine2_host.h"
 #include "engine_host.h"
 
 using namespace lbm;
 
-static int check_params2d(lbm_ctx *ctx, const lbm_params2d &p)
+int check_params2d(lbm_ctx *ctx, const lbm_params2d &p)
 {
     if (!(p.tau > 0.5)) return lbm_fail_input(ctx, "tau must exceed 0.5");
     // LMB2d/main.cpp:304
@@ -23,7 +24,7 @@ static int check_params2d(lbm_ctx *ctx, const lbm_params2d &p)
     return LBM_OK;
 }
 
-static void fill_solve2(Solve2 &S, int nx, int ny, const double F[2], const lbm_params2d &p)
+void fill_solve2(Solve2 &S, int nx, int ny, const double F[2], const lbm_params2d &p)
 {
     memset(&S, 0, sizeof(S));
     S.nx = nx; S.ny = ny; S.wpr = (nx + 31) / 32;
@@ -40,7 +41,7 @@ static void fill_solve2(Solve2 &S, int nx, int ny, const double F[2], const lbm_
     c.avg_steps = p.avg_steps; c.avg_sample = p.avg_sample; c.hold = p.hold;
 }
 
-static void init_state2(State2 &st, const Ctl2 &c)
+void init_state2(State2 &st, const Ctl2 &c)
 {
     memset(&st, 0, sizeof(st));
     st.phase = PH_RUN;

@@ -143,6 +143,30 @@ int lbm_solve2d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny,
                 int ndir, const double *forces, const lbm_params2d *params,
                 lbm_result2d *results, float *vel_out);
 
+/* Largest input of lbm_solve2d_noalloc: the reference's fixed 256 x 256 cell
+ * (LMB2d/lbm.h:24-26) and its two forcing directions (LMB2d/main.cpp:323-324). */
+#define LBM_NOALLOC2D_MAX_CELLS 65536
+#define LBM_NOALLOC2D_MAX_DIRS  2
+
+/* lbm_solve2d that allocates no device memory.  No counterpart in the
+ * reference (whose 2D solver keeps its lattice in static arrays,
+ * LMB2d/lbm.cpp:18-28; this entry point keeps that property on the device).
+ * Same arguments, codes and results (bit for bit) as lbm_solve2d, for callers
+ * that must not allocate: device memory already owned by another allocator,
+ * or a loop that cannot take the synchronisation of cudaFree.  Lattices, mask
+ * and controller state live in one static device array of this library
+ * (about 7 MB per device, reserved when the library's device code is loaded).
+ *   nx * ny > LBM_NOALLOC2D_MAX_CELLS or ndir > LBM_NOALLOC2D_MAX_DIRS:
+ * LBM_EINPUT, with lbm_last_error naming the limit.
+ *   The first call on a device looks up the array (cudaGetSymbolAddress), which
+ * may load the library's device code there: make it before any stream
+ * capture.  The call synchronises its stream and is not capturable.
+ *   One array per device and process: overlapping calls on one device would
+ * race on it, so they are serialised by a per-device lock. */
+int lbm_solve2d_noalloc(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny,
+                        int ndir, const double *forces, const lbm_params2d *params,
+                        lbm_result2d *results, float *vel_out);
+
 /* ---- batched / served solves ------------------------------------------ */
 typedef struct lbm_batch lbm_batch;
 
