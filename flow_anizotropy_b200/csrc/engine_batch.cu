@@ -1,10 +1,13 @@
 // liblbm batch engine: many resident 3D solves of one storage precision,
-// advanced together.  One persistent step kernel per time step walks a device
-// work list of (solve, tile) items covering every unfinished solve, each at
-// its own step count; a chunk of steps is one CUDA graph launch.  Solves
-// retire on the device (the controller marks them done) and are reclaimed by
-// lbm_batch_poll; new structures can be admitted between chunks, which is
-// what the serving loop uses for continuous batching.
+// advanced together.  One step kernel per time step covers a device work list
+// of (solve, tile) items of every unfinished solve, each at its own step
+// count, one block per item (the hardware block scheduler balances tiles of
+// uneven cost, and blocks running at the same time touch neighbouring
+// tiles); a chunk of steps is one CUDA graph launch.  When the work list
+// changes, the graph's launch sizes are updated in place.  Solves retire on
+// the device (the controller marks them done; their blocks exit at once) and
+// are reclaimed by lbm_batch_poll; new structures can be admitted between
+// chunks, which is what the serving loop uses for continuous batching.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,8 +51,8 @@ struct lbm_batch {
     long long resident = 0;
     int cap_slots = 0;
     int cap_work = 0;
-    int grid = 0;          // persistent grid of the even-step (or moment) kernel
-    int grid_odd = 0;      // persistent grid of the odd-step kernel
+    int nwork = 0;         // items in the device work list (= blocks per step launch)
+    int graph_nwork = -1;  // launch size the graph holds
     std::vector<Slot> slots;
     DevMem d_solves{nullptr}, d_states{nullptr}, d_work{nullptr}, d_nwork{nullptr};
     cudaGraph_t graph = nullptr;
@@ -66,16 +69,17 @@ static void destroy_graph(lbm_batch *b)
 }
 
 // One graph = `chunk` step launches (step index 0..chunk-1 relative to each
-// solve's s_base) followed by the s_base advance.
+// solve's s_base) followed by the s_base advance.  An existing executable
+// graph is updated in place when only launch sizes changed.
 static int capture(lbm_batch *b)
 {
     lbm_ctx *ctx = b->ctx;
-    destroy_graph(b);
     StepArgs a;
     a.solves = static_cast<const Solve3 *>(b->d_solves.p);
     a.work = static_cast<const int2 *>(b->d_work.p);
     a.nwork_dev = static_cast<const int *>(b->d_nwork.p);
     a.nwork = 0;
+    const dim3 grid(std::max(1, b->nwork));
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     // chunks are even and solves join at chunk boundaries (s_base even), so
@@ -83,8 +87,7 @@ static int capture(lbm_batch *b)
     for (int i = 0; i < b->chunk && e == cudaSuccess; ++i) {
         a.step = i;
         const bool odd = ((i + 1) & 1) == 1;
-        a.nwork = 0;
-        e = lbm_launch_step(b->precision, b->variant, b->w1, odd, dim3(odd ? b->grid_odd : b->grid), ctx->stream, a);
+        e = lbm_launch_step(b->precision, b->variant, b->w1, odd, grid, ctx->stream, a);
     }
     if (e == cudaSuccess) {
         advance3d_kernel<<<(b->cap_slots + 255) / 256, 256, 0, ctx->stream>>>(
@@ -95,8 +98,20 @@ static int capture(lbm_batch *b)
     cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);
     if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return lbm_fail_cuda(ctx, e, "graph capture", __LINE__); }
     CK(e2);
+    if (b->exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(b->exec, g, &info) == cudaSuccess) {
+            if (b->graph) cudaGraphDestroy(b->graph);
+            b->graph = g;
+            b->graph_nwork = b->nwork;
+            return LBM_OK;
+        }
+        cudaGetLastError();            // not updatable (kernels changed): instantiate anew
+    }
+    destroy_graph(b);
     b->graph = g;
     CK(cudaGraphInstantiate(&b->exec, g, 0));
+    b->graph_nwork = b->nwork;
     return LBM_OK;
 }
 
@@ -118,13 +133,18 @@ static int sync_work(lbm_batch *b)
         if (!s.retired)
             for (int t = 0; t < s.S.ntiles; ++t) work.push_back(make_int2(i, t));
     }
-    if ((int)work.size() > b->cap_work) {
-        b->cap_work = std::max<int>((int)work.size(), 2 * b->cap_work);
+    const int nwork = (int)work.size();
+    bool recapture = nwork != b->graph_nwork;
+    if (nwork > b->cap_work) {
+        b->cap_work = std::max<int>(nwork, 2 * b->cap_work);
         CK(b->d_work.alloc(sizeof(int2) * (size_t)b->cap_work));
+        recapture = true;
+    }
+    b->nwork = nwork;
+    if (recapture) {
         int rc = capture(b);
         if (rc) return rc;
     }
-    const int nwork = (int)work.size();
     CK(cudaMemcpyAsync(b->d_solves.p, desc.data(), sizeof(Solve3) * b->cap_slots, cudaMemcpyHostToDevice, ctx->stream));
     if (nwork)
         CK(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, ctx->stream));
@@ -175,11 +195,7 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     std::vector<State3> done(b->cap_slots);
     for (auto &st : done) { memset(&st, 0, sizeof(st)); st.phase = PH_DONE; }
     CK(cudaMemcpyAsync(b->d_states.p, done.data(), sizeof(State3) * b->cap_slots, cudaMemcpyHostToDevice, ctx->stream));
-    b->grid = ctx->sms * std::max(1, lbm_max_blocks(precision, b->variant, false));
-    b->grid_odd = ctx->sms * std::max(1, lbm_max_blocks(precision, b->variant, true));
     int rc = sync_work(b.get());
-    if (rc) return rc;
-    rc = capture(b.get());
     if (rc) return rc;
     *out = b.release();
     return LBM_OK;
