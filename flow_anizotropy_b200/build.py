@@ -29,6 +29,7 @@ UNITS = {
     "k2d.cu": ["-fmad=false"],
     "k3d_lp.cu": [],
     "k3d_m.cu": [],
+    "k3d_md.cu": [],
     "engine.cu": [],
     "engine2.cu": [],
     "engine2_noalloc.cu": [],

@@ -15,6 +15,7 @@
 #include "engine2d.cuh"
 #include "engine_host.h"
 #include "engine_m.cuh"
+#include "engine_md.cuh"
 
 using namespace lbm;
 
@@ -148,8 +149,8 @@ int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
 {
     if (!(p.tau > 0.5)) return lbm_fail_input(ctx, "tau must exceed 0.5");
     if (p.lag <= 0) return lbm_fail_input(ctx, "--lag must be positive");
-    if (p.precision < LBM_FP64 || p.precision > LBM_M64) return lbm_fail_input(ctx, "unknown precision");
-    if (is_moment(p.precision) && p.tau != 1.0)
+    if (p.precision < LBM_FP64 || p.precision > LBM_MD32) return lbm_fail_input(ctx, "unknown precision");
+    if ((is_moment(p.precision) || is_dense_m(p.precision)) && p.tau != 1.0)
         return lbm_fail_input(ctx, "moment-projected storage needs tau = 1");
     if (p.criterion != LBM_CRIT_DRIFT && p.criterion != LBM_CRIT_BLOCK) return lbm_fail_input(ctx, "unknown criterion");
     if (p.criterion == LBM_CRIT_BLOCK && (p.sample <= 0 || p.lag % p.sample != 0))
@@ -170,6 +171,12 @@ long long lbm_lattice_bytes3d(long long n, int prec)
     return (long long)Q3 * lbm_plane_elems(n) * (long long)elem_size(prec);
 }
 
+// Lattice bytes of one direction of a filled solve record.
+long long lbm_lattice_bytes(const Solve3 &S)
+{
+    return is_dense_m(S.prec) ? md_lattice_bytes(S.md) : lbm_lattice_bytes3d(S.nfluid, S.prec);
+}
+
 // Plane stride (populations) or record slots per buffer (moments).
 long long lbm_plane_for(int prec, long long n)
 {
@@ -179,7 +186,7 @@ long long lbm_plane_for(int prec, long long n)
 // A variant whose even kernel reads neighbour records needs them built.
 int lbm_effective_variant(int prec, int variant, bool have_meta)
 {
-    if (is_moment(prec) || have_meta) return variant;
+    if (is_moment(prec) || is_dense_m(prec) || have_meta) return variant;
     const int ve = variant % NVAR_EVEN;
     if (!even_meta(ve)) return variant;
     return variant - ve + (ve & 1) + 2;                 // same budget, ranks from the mask
@@ -188,23 +195,27 @@ int lbm_effective_variant(int prec, int variant, bool have_meta)
 cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
     if (prec == LBM_FP64) return launch_step3d_f64(variant, odd, grid, s, a);
+    if (is_dense_m(prec)) return launch_stepmd(variant, grid, s, a);
     if (is_moment(prec)) return launch_stepm(prec, variant, grid, s, a);
     return launch_step3d_lp(prec, variant, w1, odd, grid, s, a);
 }
 
 int lbm_max_blocks(int prec, int variant, bool odd)
 {
+    if (is_dense_m(prec)) return max_blocks_stepmd(variant);
     return is_moment(prec) ? max_blocks_stepm(prec, variant) : max_blocks_step3d(prec, variant, odd);
 }
 
 cudaError_t lbm_init_lattice(int prec, const Solve3 &S, cudaStream_t s)
 {
+    if (is_dense_m(prec)) return init_md_lattice(S, s);   // tensor maps; step 1 writes the records
     if (is_moment(prec)) return cudaSuccess;        // step 1 writes the moments from scratch
     return launch_init3d(prec, S.A, S.plane, S.nfluid, s);
 }
 
 cudaError_t lbm_canon(int prec, const Solve3 &S, long long done, double *f, float *u, cudaStream_t s)
 {
+    if (is_dense_m(prec)) return launch_canonmd(S, done, f, u, s);
     if (is_moment(prec)) return launch_canonm(prec, S, done, f, u, s);
     return launch_canon3d(prec, S, done, f, u, s);
 }
@@ -218,6 +229,7 @@ void lbm_fill_solve3(Solve3 &S, int nx, int ny, int nz, const double F[3], const
     S.nn = (long long)nx * ny * nz;
     S.plane = lbm_plane_elems(S.nn);
     S.ntiles = (int)((S.nn + TPB * npt - 1) / (TPB * npt));
+    if (is_dense_m(p.precision)) md_fill_geom(S.md, nx, ny, nz, p.variant, S.ntiles);
     S.dvx.init(nx);
     S.dvy.init(ny);
     Phys3 &P = S.P;
@@ -291,6 +303,16 @@ int lbm_build_pores(lbm_ctx *ctx, Solve3 &S, int npt, DevMem &wpre, DevMem &fnod
     S.wpre = static_cast<const uint32_t *>(wpre.p);
     S.fnode = static_cast<const uint32_t *>(fnode.p);
     S.nfluid = (int)total;
+    if (is_dense_m(S.prec)) {
+        // dense moment form: tiles cover the box; the padded byte mask
+        // replaces the neighbour records
+        S.meta = nullptr;
+        S.meta2 = nullptr;
+        CK(meta.alloc((size_t)md_pmask_bytes(S.md, S.ny, S.nz)));
+        S.md.pmask = static_cast<const uint8_t *>(meta.p);
+        CK(launch_padmask(S, ctx->stream));
+        return LBM_OK;
+    }
     S.plane = lbm_plane_for(S.prec, (long long)total);
     S.ntiles = (int)((total + (unsigned long long)TPB * npt - 1) / ((unsigned long long)TPB * npt));
     if (S.ntiles == 0) S.ntiles = 1;
@@ -315,6 +337,7 @@ void lbm_copy_pores(Solve3 &dst, const Solve3 &src)
     dst.wpre = src.wpre; dst.fnode = src.fnode; dst.nfluid = src.nfluid;
     dst.meta = src.meta; dst.meta2 = src.meta2;
     dst.plane = src.plane; dst.ntiles = src.ntiles;
+    dst.md.pmask = src.md.pmask;
 }
 
 // Run a set of 3D solves sharing one mask to completion, one launch per step.
@@ -395,7 +418,7 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
         lbm_copy_pores(S, proto);
         lat.emplace_back(ctx->stream);
         part.emplace_back(ctx->stream);
-        CK(lat.back().alloc((size_t)lbm_lattice_bytes3d(S.nfluid, prec)));
+        CK(lat.back().alloc((size_t)lbm_lattice_bytes(S)));
         CK(part.back().alloc(sizeof(double) * 3 * (size_t)S.ntiles));
         S.A = lat.back().p;
         S.mask = static_cast<const uint32_t *>(mask.p);
@@ -482,7 +505,7 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     S.mask = static_cast<const uint32_t *>(mask.p);
     rc = lbm_build_pores(ctx, S, npt, wpre, fnode, meta, meta2);
     if (rc) return rc;
-    CK(lat.alloc((size_t)lbm_lattice_bytes3d(S.nfluid, precision)));
+    CK(lat.alloc((size_t)lbm_lattice_bytes(S)));
     CK(part.alloc(sizeof(double) * 3 * (size_t)S.ntiles));
     CK(d_states.alloc(sizeof(State3)));
     S.A = lat.p; S.mask = static_cast<const uint32_t *>(mask.p);
@@ -518,7 +541,7 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
 
 extern "C" int lbm_variant_count(int precision)
 {
-    return (precision >= LBM_FP64 && precision <= LBM_M64) ? variant_count(precision) : 0;
+    return (precision >= LBM_FP64 && precision <= LBM_MD32) ? variant_count(precision) : 0;
 }
 
 // Autotuner: every variant runs the same fixed number of steps on the same
@@ -530,7 +553,7 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
     if (!ctx) return LBM_EINPUT;
     CK(cudaSetDevice(ctx->device));
     if (nx <= 0 || ny <= 0 || nz <= 0 || ndir <= 0 || nsteps <= 0) return lbm_fail_input(ctx, "bad arguments");
-    if (precision < LBM_FP64 || precision > LBM_M64) return lbm_fail_input(ctx, "unknown precision");
+    if (precision < LBM_FP64 || precision > LBM_MD32) return lbm_fail_input(ctx, "unknown precision");
     const long long nn = (long long)nx * ny * nz;
     if (nn >= (1ll << 31) || (long long)Q3 * lbm_plane_elems(nn) >= (1ll << 32))
         return lbm_fail_input(ctx, "lattice too large");
@@ -539,16 +562,29 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
     int rc = lbm_upload_mask(ctx, solid, nx, (long long)ny * nz, mask, npore);
     if (rc) return rc;
     const int nv = variant_count(precision);
+    // lattice bytes and tile count bounds over the variants
+    long long lat_bytes = 0, max_tiles = (nn + TPB - 1) / TPB + 1;
+    for (int v = 0; v < nv; ++v) {
+        lbm_params3d pv;
+        memset(&pv, 0, sizeof(pv));
+        pv.tau = 1.0; pv.precision = precision; pv.variant = v;
+        Solve3 g;
+        const double F0[3] = {0, 0, 0};
+        lbm_fill_solve3(g, nx, ny, nz, F0, pv, variant_npt(precision, v));
+        g.nfluid = (int)npore;
+        lat_bytes = std::max(lat_bytes, lbm_lattice_bytes(g));
+        max_tiles = std::max<long long>(max_tiles, g.ntiles);
+    }
     std::vector<DevMem> lat;
     lat.reserve(ndir);
     for (int j = 0; j < ndir; ++j) {
         lat.emplace_back(ctx->stream);
-        CK(lat.back().alloc((size_t)lbm_lattice_bytes3d(npore, precision)));
+        CK(lat.back().alloc((size_t)lat_bytes));
     }
     DevMem d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream), part(ctx->stream);
     CK(d_states.alloc(sizeof(State3) * ndir));
     CK(d_solves.alloc(sizeof(Solve3) * ndir));
-    CK(part.alloc(sizeof(double) * 3 * (size_t)((nn + TPB - 1) / TPB + 1) * ndir));
+    CK(part.alloc(sizeof(double) * 3 * (size_t)max_tiles * ndir));
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -577,7 +613,7 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
             lbm_copy_pores(hs[j], proto);
             hs[j].A = lat[j].p;
             hs[j].mask = proto.mask;
-            hs[j].partials = static_cast<double *>(part.p) + 3ll * j * ((nn + TPB - 1) / TPB + 1);
+            hs[j].partials = static_cast<double *>(part.p) + 3ll * j * max_tiles;
             hs[j].st = static_cast<State3 *>(d_states.p) + j;
             lbm_init_state3(hst[j], hs[j].c);
             CK(lbm_init_lattice(precision, hs[j], ctx->stream));

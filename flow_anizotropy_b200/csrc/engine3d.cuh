@@ -93,6 +93,16 @@ struct State3 {
     long long avg_start;  // step at which phase 1 ended
 };
 
+// Geometry of the dense moment form (LBM_MD32): a record for every voxel in
+// a padded volume with one ghost layer per face (periodic images), rows
+// padded to 16 bytes so that TMA boxes start on aligned addresses.
+struct MDGeom {
+    const uint8_t *pmask;  // padded byte mask (1 = solid), xpm x (ny+2) x (nz+2)
+    long long vol;         // cells of one record component: xp * (ny+2) * (nz+2)
+    int xp, xpm;           // padded row lengths: records (floats), mask (bytes)
+    int nxt, nyt, nzs, lz; // tiles along x and y, z segments of lz planes
+};
+
 struct Solve3 {
     void *A;
     long long plane;         // elements per plane (>= nfluid)
@@ -112,6 +122,7 @@ struct Solve3 {
     Ctl3 c;
     double *partials;     // ntiles * 3
     State3 *st;
+    MDGeom md;            // dense moment form only
 };
 
 struct StepArgs {
@@ -710,7 +721,12 @@ cudaError_t launch_init3d(int prec, void *A, long long plane, long long n, cudaS
 cudaError_t launch_canon3d(int prec, const Solve3 &S, long long done, double *f, float *u, cudaStream_t s);
 int max_blocks_step3d(int prec, int variant, bool odd);
 inline bool is_moment(int prec) { return prec == 4 || prec == 5; }
-inline int variant_count(int prec) { return prec == 0 ? NVAR_F64 : (prec >= 4 ? 3 : NVAR_LP); }
+inline bool is_dense_m(int prec) { return prec == 6; }
+// Dense moment form variants: z-segment length (planes per tile) x
+// shared-memory ring depth x register budget.
+constexpr int NVAR_MD = 4;
+__host__ __device__ constexpr int md_lz(int v) { return v == 1 ? 32 : v == 2 ? 8 : 16; }
+inline int variant_count(int prec) { return prec == 0 ? NVAR_F64 : prec == 6 ? NVAR_MD : (prec >= 4 ? 3 : NVAR_LP); }
 // pore voxels per tile (in units of TPB) of a solve's tile list
 inline int variant_npt(int prec, int) { return prec >= 4 ? 1 : TILE_NPT; }
 

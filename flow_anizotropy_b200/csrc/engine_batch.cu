@@ -18,6 +18,7 @@
 
 #include "../../include/lbm.h"
 #include "engine3d.cuh"
+#include "engine_md.cuh"
 #include "engine_host.h"
 
 using namespace lbm;
@@ -159,6 +160,12 @@ extern "C" long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int pre
     const long long nn = (long long)nx * ny * nz;
     // upper bound: every voxel a pore (the batch charges the exact size on admission)
     const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 28ll * nn + 8;
+    if (is_dense_m(precision)) {
+        MDGeom g{};
+        int tiles = 0;
+        md_fill_geom(g, nx, ny, nz, 0, tiles);
+        return tables + md_pmask_bytes(g, ny, nz) + (long long)ndir * (md_lattice_bytes(g) + 24ll * tiles);
+    }
     const long long tiles = (nn + TPB - 1) / TPB;
     return tables + (long long)ndir * (lbm_lattice_bytes3d(nn, precision) + 24 * tiles);
 }
@@ -168,7 +175,7 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     if (!ctx || !out) return LBM_EINPUT;
     *out = nullptr;
     CK(cudaSetDevice(ctx->device));
-    if (precision < LBM_FP64 || precision > LBM_M64) return lbm_fail_input(ctx, "unknown precision");
+    if (precision < LBM_FP64 || precision > LBM_MD32) return lbm_fail_input(ctx, "unknown precision");
     if (chunk <= 0 || chunk > 4096) return lbm_fail_input(ctx, "chunk must be in 1..4096");
     chunk += chunk & 1;                  // even: every solve keeps the launch's parity
     if (hbm_budget <= 0) return lbm_fail_input(ctx, "budget must be positive");
@@ -249,8 +256,9 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         if (rc) return rc;
     }
     const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 4ll * proto.nfluid + 8 +
-                             (proto.meta ? 24ll * proto.nfluid : 0);
-    const long long exact = tables + (long long)ndir * (lbm_lattice_bytes3d(proto.nfluid, b->precision) + 24ll * proto.ntiles);
+                             (proto.meta ? 24ll * proto.nfluid : 0) +
+                             (is_dense_m(b->precision) ? md_pmask_bytes(proto.md, ny, nz) : 0);
+    const long long exact = tables + (long long)ndir * (lbm_lattice_bytes(proto) + 24ll * proto.ntiles);
     if (b->resident + exact > b->budget) {
         ctx->err = "batch budget exhausted";
         return LBM_EBUSY;
@@ -268,7 +276,7 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         lbm_copy_pores(s.S, proto);
         s.wpre = wpre; s.fnode = fnode; s.meta = meta; s.meta2 = meta2;
         s.tables = tables;
-        CK(s.lattice.alloc((size_t)lbm_lattice_bytes3d(s.S.nfluid, b->precision)));
+        CK(s.lattice.alloc((size_t)lbm_lattice_bytes(s.S)));
         CK(s.partials.alloc(sizeof(double) * 3 * (size_t)s.S.ntiles));
         s.S.A = s.lattice.p;
         s.S.mask = static_cast<const uint32_t *>(mask->p);
@@ -279,7 +287,7 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         s.dir = j;
         s.used = true;
         s.retired = false;
-        s.bytes = lbm_lattice_bytes3d(s.S.nfluid, b->precision) + 24ll * s.S.ntiles;
+        s.bytes = lbm_lattice_bytes(s.S) + 24ll * s.S.ntiles;
         lbm_init_state3(init[j], s.S.c);
         CK(lbm_init_lattice(b->precision, s.S, ctx->stream));
         CK(cudaMemcpyAsync(s.S.st, &init[j], sizeof(State3), cudaMemcpyHostToDevice, ctx->stream));

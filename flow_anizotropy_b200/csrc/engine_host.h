@@ -57,6 +57,8 @@ int lbm_upload_mask(lbm_ctx *ctx, const uint8_t *solid, int nx, long long rows, 
 int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p);
 long long lbm_plane_elems(long long nn);
 long long lbm_lattice_bytes3d(long long nn, int prec);
+// Lattice bytes of one direction of a filled solve record (any storage form).
+long long lbm_lattice_bytes(const lbm::Solve3 &S);
 void lbm_fill_solve3(lbm::Solve3 &S, int nx, int ny, int nz, const double F[3], const lbm_params3d &p, int npt);
 void lbm_init_state3(lbm::State3 &st, const lbm::Ctl3 &c);
 int lbm_pick_npt(const lbm_params3d &p);

@@ -191,6 +191,11 @@ def debug_steps2d(solid, force, nsteps, tau=1.0, device=0):
     return f, u, np.array(q[:])
 
 
+def variant_count(precision="fp32") -> int:
+    """Number of step-kernel variants of a storage precision."""
+    return int(_lib.load().lbm_variant_count(_lib.PRECISIONS[precision]))
+
+
 def tune3d(solid, ndir=3, precision="fp32", nsteps=200, device=0):
     """Time every step-kernel variant on this structure; returns (best, ms_per_step list)."""
     ctx = _lib.context(device)

@@ -52,6 +52,8 @@ extern "C" {
  * rounding at the storage precision). */
 #define LBM_M32   4   /* moments as float, FP32 arithmetic                       */
 #define LBM_M64   5   /* moments as double, FP64 arithmetic                      */
+#define LBM_MD32  6   /* moments as float over the dense voxel box, z-planes    */
+                      /* staged in shared memory by TMA                          */
 
 /* Phase-1 convergence criterion */
 #define LBM_CRIT_DRIFT  0  /* every lag steps: max_c |q_c - qprev_c| < eps ||q||
