@@ -187,9 +187,28 @@ long long lbm_plane_for(int prec, long long n)
 int lbm_effective_variant(int prec, int variant, bool have_meta)
 {
     if (is_moment(prec) || is_dense_m(prec) || have_meta) return variant;
-    const int ve = variant % NVAR_EVEN;
+    const int ve = variant % nvar_even(prec);
     if (!even_meta(ve)) return variant;
+    if (even_grouped(ve)) return variant - ve + 6;      // grouped, ranks from the mask
     return variant - ve + (ve & 1) + 2;                 // same budget, ranks from the mask
+}
+
+// Does this (effective) variant run the grouped even kernel?
+static bool lbm_grouped_variant(int prec, int variant)
+{
+    return prec >= LBM_FP32 && prec <= LBM_BF16 && even_grouped(variant % NVAR_EVEN_LP);
+}
+
+// Work list of the grouped even step over solves that share one structure:
+// runs of up to MAX_GROUP consecutive records, led by the first of each run.
+static void lbm_group_items(std::vector<Solve3> &hs, std::vector<int2> &items)
+{
+    const int n = (int)hs.size();
+    for (auto &S : hs) S.group = 0;
+    for (int j = 0; j < n; j += MAX_GROUP) {
+        hs[j].group = std::min(MAX_GROUP, n - j);
+        for (int t = 0; t < hs[j].ntiles; ++t) items.push_back(make_int2(j, t));
+    }
 }
 
 cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
@@ -353,6 +372,17 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
     long long s = 0;
     StepArgs a;
     a.solves = d_solves; a.work = d_work; a.nwork_dev = nullptr; a.nwork = nwork;
+    StepArgs ae = a;                  // even steps (grouped work list for grouped variants)
+    DevMem gwork(ctx->stream);
+    if (lbm_grouped_variant(prec, variant)) {
+        std::vector<int2> items;
+        lbm_group_items(hs, items);
+        CK(gwork.alloc(sizeof(int2) * items.size()));
+        CK(cudaMemcpyAsync(gwork.p, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(d_solves, hs.data(), sizeof(Solve3) * n, cudaMemcpyHostToDevice, ctx->stream));
+        ae.work = static_cast<const int2 *>(gwork.p);
+        ae.nwork = (int)items.size();
+    }
     for (;;) {
         CK(cudaMemcpyAsync(hst.data(), d_states, sizeof(State3) * n, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -370,9 +400,11 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
         }
         if (target == LLONG_MAX) break;
         for (; s < target; ++s) {
-            a.step = s;
             // every solve of the call is at step s + 1 (they start together)
-            CK(lbm_launch_step(prec, variant, w1, ((s + 1) & 1) == 1, dim3(nwork), ctx->stream, a));
+            const bool odd = ((s + 1) & 1) == 1;
+            StepArgs &x = odd ? a : ae;
+            x.step = s;
+            CK(lbm_launch_step(prec, variant, w1, odd, dim3(x.nwork), ctx->stream, x));
         }
     }
     return LBM_OK;
@@ -630,9 +662,22 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
         a.nwork_dev = nullptr;
         a.nwork = (int)work.size();
         const int ev = lbm_effective_variant(precision, v, proto.meta != nullptr);
+        StepArgs ae = a;
+        DevMem gw(ctx->stream);
+        if (lbm_grouped_variant(precision, ev)) {
+            std::vector<int2> items;
+            lbm_group_items(hs, items);
+            CK(gw.alloc(sizeof(int2) * items.size()));
+            CK(cudaMemcpyAsync(gw.p, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(d_solves.p, hs.data(), sizeof(Solve3) * ndir, cudaMemcpyHostToDevice, ctx->stream));
+            ae.work = static_cast<const int2 *>(gw.p);
+            ae.nwork = (int)items.size();
+        }
         auto launch = [&](long long s) {
-            a.step = s;
-            return lbm_launch_step(precision, ev, true, ((s + 1) & 1) == 1, dim3(a.nwork), ctx->stream, a);
+            const bool odd = ((s + 1) & 1) == 1;
+            StepArgs &x = odd ? a : ae;
+            x.step = s;
+            return lbm_launch_step(precision, ev, true, odd, dim3(x.nwork), ctx->stream, x);
         };
         long long s = 0;
         for (int i = 0; i < std::max(2, nsteps / 4); ++i) CK(launch(s++));

@@ -123,6 +123,7 @@ struct Solve3 {
     double *partials;     // ntiles * 3
     State3 *st;
     MDGeom md;            // dense moment form only
+    int group;            // grouped even step: directions in the group led by this record (else 0)
 };
 
 struct StepArgs {
@@ -413,21 +414,27 @@ __device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, const uin
 // register budgets: the odd (local) step is pure streaming and wants many
 // loads in flight (several voxels per thread, high occupancy); the even
 // (neighbour) step carries the neighbour-rank arithmetic.  A variant index
-// v selects odd variant v / NVAR_EVEN and even variant v % NVAR_EVEN;
-// lbm_tune3d times them on the actual structure.
+// v selects odd variant v / NVAR_EVEN and even variant v % NVAR_EVEN
+// (NVAR_EVEN_LP for the reduced-precision storage, which adds the grouped
+// even kernels); lbm_tune3d times them on the actual structure.
 struct Variant { int npt, minb; };
-constexpr int NVAR_ODD = 3, NVAR_EVEN = 6;
-constexpr int NVAR_LP = NVAR_ODD * NVAR_EVEN, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
+constexpr int NVAR_ODD = 3, NVAR_EVEN = 6, NVAR_EVEN_LP = 8;
+constexpr int NVAR_LP = NVAR_ODD * NVAR_EVEN_LP, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
+constexpr int MAX_GROUP = 3;    // directions per grouped even step
+inline int nvar_even(int prec) { return prec == 0 ? NVAR_EVEN : NVAR_EVEN_LP; }
 __host__ __device__ constexpr Variant odd_lp(int v) { return v == 0 ? Variant{1, 4} : v == 1 ? Variant{1, 5} : Variant{2, 2}; }
 // even variants: 0-1 read the neighbour record (META), 2-3 compute ranks from
-// the mask, 4-5 read the record and stage their gathers with cp.async
+// the mask, 4-5 read the record and stage their gathers with cp.async, 6-7
+// are grouped (one rank computation for all directions of a structure; 6
+// from the mask, 7 from the record)
 __host__ __device__ constexpr Variant even_lp(int v)
 {
     return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : v == 2 ? Variant{1, 3} : v == 3 ? Variant{1, 4}
-         : v == 4 ? Variant{1, 4} : Variant{1, 3};
+         : v == 4 ? Variant{1, 4} : v == 5 ? Variant{1, 3} : Variant{1, 2};
 }
-__host__ __device__ constexpr bool even_meta(int v) { return v < 2 || v >= 4; }
-__host__ __device__ constexpr bool even_async(int v) { return v >= 4; }
+__host__ __device__ constexpr bool even_meta(int v) { return v < 2 || v == 4 || v == 5 || v == 7; }
+__host__ __device__ constexpr bool even_async(int v) { return v == 4 || v == 5; }
+__host__ __device__ constexpr bool even_grouped(int v) { return v >= 6; }
 __host__ __device__ constexpr Variant odd_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{2, 1} : Variant{1, 1}; }
 __host__ __device__ constexpr Variant even_f64(int v)
 {
@@ -559,6 +566,99 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
         if (red) finish_tile(S, item.y, n, acc, sh);
+    }
+}
+
+// Even step of a group of directions that share one structure (consecutive
+// solve records; the first holds the group size in `group`): the neighbour
+// ranks of a pore voxel are found once and serve every direction's lattice,
+// and the gathers of one direction overlap the rank work of the next voxel.
+// Per-direction phases, step counts and reductions are those of
+// step3d_even_kernel, with the flux partials summed in the same order, so the
+// results are bit-identical to it.
+template <class ST, int MINB, bool W1, bool META>
+__global__ void __launch_bounds__(TPB, MINB) step3d_even_group_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    using Cp = typename ST::C;
+    __shared__ double sh[TPB / 32][3];
+    __shared__ double sacc[MAX_GROUP][3][TPB];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S0 = a.solves[item.x];
+        const int ng = min(S0.group, MAX_GROUP);
+        unsigned live = 0, redm = 0;
+#pragma unroll
+        for (int d = 0; d < MAX_GROUP; ++d) {
+            if (d >= ng) break;
+            const Solve3 &S = a.solves[item.x + d];
+            const int phase = S.st->phase;
+            if (phase >= PH_DONE) continue;
+            live |= 1u << d;
+            if (needs_reduction(S.c, phase, S.st->s_base + a.step + 1)) {
+                redm |= 1u << d;
+                sacc[d][0][threadIdx.x] = 0.0;
+                sacc[d][1][threadIdx.x] = 0.0;
+                sacc[d][2][threadIdx.x] = 0.0;
+            }
+        }
+        if (!live) continue;
+        const unsigned P = (unsigned)S0.plane;
+#pragma unroll 1
+        for (int j = 0; j < TILE_NPT; ++j) {
+            const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
+            if (i >= (unsigned)S0.nfluid) continue;
+            CNb nb;
+            if constexpr (META) {
+                meta_nbrs(S0, i, __ldg(S0.meta + i), __ldg(S0.meta2 + i), nb);
+            } else {
+                int x, y, z;
+                coords3(S0, __ldg(S0.fnode + i), x, y, z);
+                compact_nbrs(S0, i, x, y, z, nb);
+            }
+            // every direction's pulls are issued before the first collision:
+            // one memory round trip serves all the directions of the voxel
+            Cp g[MAX_GROUP][Q3];
+#pragma unroll
+            for (int d = 0; d < MAX_GROUP; ++d) {
+                if (!((live >> d) & 1u)) continue;
+                const T *__restrict__ A = static_cast<const T *>(a.solves[item.x + d].A);
+                g[d][0] = ST::ld(A + i);
+#pragma unroll
+                for (int k = 1; k < Q3; ++k) {
+                    const int o = opp3(k);
+                    const unsigned src = ((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]);
+                    g[d][k] = ST::ld(A + src);
+                }
+            }
+#pragma unroll
+            for (int d = 0; d < MAX_GROUP; ++d) {
+                if (!((live >> d) & 1u)) continue;
+                const Solve3 &S = a.solves[item.x + d];
+                T *__restrict__ A = static_cast<T *>(S.A);
+                Cp ux, uy, uz;
+                collide3<ST, W1>(g[d], S, ux, uy, uz);
+                ST::st(A + i, g[d][0]);
+#pragma unroll
+                for (int k = 1; k < Q3; ++k) {
+                    const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
+                    ST::st(A + dst, g[d][k]);
+                }
+                if ((redm >> d) & 1u) {
+                    sacc[d][0][threadIdx.x] += (double)ux;
+                    sacc[d][1][threadIdx.x] += (double)uy;
+                    sacc[d][2][threadIdx.x] += (double)uz;
+                }
+            }
+        }
+#pragma unroll 1
+        for (int d = 0; d < ng; ++d) {
+            if (!((redm >> d) & 1u)) continue;
+            const Solve3 &S = a.solves[item.x + d];
+            double acc[3] = {sacc[d][0][threadIdx.x], sacc[d][1][threadIdx.x], sacc[d][2][threadIdx.x]};
+            finish_tile(S, item.y, S.st->s_base + a.step + 1, acc, sh);
+        }
     }
 }
 

@@ -11,12 +11,13 @@ int max_blocks_f64(int variant, bool odd);
 #define LBM_ODD(ST, V, W) step3d_odd_kernel<ST, odd_lp(V).npt, odd_lp(V).minb, W>
 #define LBM_EVEN(ST, V, W) step3d_even_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 #define LBM_EVENA(ST, V, W) step3d_even_async_kernel<ST, even_lp(V).minb, W>
+#define LBM_EVENG(ST, V, W) step3d_even_group_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 
 template <class ST, bool W>
 static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
     if (v < 0 || v >= NVAR_LP) return cudaErrorInvalidValue;
-    const int vo = v / NVAR_EVEN, ve = v % NVAR_EVEN;
+    const int vo = v / NVAR_EVEN_LP, ve = v % NVAR_EVEN_LP;
     if (odd) {
         switch (vo) {
         case 0: LBM_ODD(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
@@ -30,7 +31,9 @@ static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const S
         case 2: LBM_EVEN(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
         case 3: LBM_EVEN(ST, 3, W)<<<grid, TPB, 0, s>>>(a); break;
         case 4: LBM_EVENA(ST, 4, W)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_EVENA(ST, 5, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 5: LBM_EVENA(ST, 5, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 6: LBM_EVENG(ST, 6, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_EVENG(ST, 7, W)<<<grid, TPB, 0, s>>>(a); break;
         }
     }
     return cudaGetLastError();
@@ -49,12 +52,13 @@ cudaError_t launch_step3d_lp(int prec, int variant, bool w1, bool odd, dim3 grid
 template <class ST>
 static int occ(int v, bool odd)
 {
-    const int vo = v / NVAR_EVEN, ve = v % NVAR_EVEN;
+    const int vo = v / NVAR_EVEN_LP, ve = v % NVAR_EVEN_LP;
     const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(ST, 0, true) : vo == 1 ? (const void *)LBM_ODD(ST, 1, true)
                                                                         : (const void *)LBM_ODD(ST, 2, true))
                         : (ve == 0 ? (const void *)LBM_EVEN(ST, 0, true) : ve == 1 ? (const void *)LBM_EVEN(ST, 1, true)
                            : ve == 2 ? (const void *)LBM_EVEN(ST, 2, true) : ve == 3 ? (const void *)LBM_EVEN(ST, 3, true)
-                           : ve == 4 ? (const void *)LBM_EVENA(ST, 4, true) : (const void *)LBM_EVENA(ST, 5, true));
+                           : ve == 4 ? (const void *)LBM_EVENA(ST, 4, true) : ve == 5 ? (const void *)LBM_EVENA(ST, 5, true)
+                           : ve == 6 ? (const void *)LBM_EVENG(ST, 6, true) : (const void *)LBM_EVENG(ST, 7, true));
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;

@@ -66,3 +66,29 @@ def test_bad_input_is_status_2(gpu):
     with pytest.raises(S.LBMError) as e:
         S.solve3d(bad, [[1e-6, 0, 0]])
     assert e.value.code == 2 and "non-binary" in str(e.value)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+@pytest.mark.parametrize("ndir", [3, 4, 1])
+def test_grouped_even_step_equals_per_direction(gpu, packing, prec, ndir):
+    """The grouped even kernels (one neighbour-rank computation for all
+    directions of a structure) give the per-direction kernels' bits: same step
+    counts, fluxes, standard errors and velocity fields, also for a fourth
+    direction (a group of one after a group of three) and a single one."""
+    F = 1e-6
+    forces = [[F, 0, 0], [0, F, 0], [0, 0, F], [F / 3**0.5] * 3][:ndir]
+    nv_even = 8
+    runs = {}
+    for ve in (2, 3, 6, 7):
+        p = S.Params3D(precision=prec, variant=ve, **PRM)
+        runs[ve] = S.solve3d(packing, forces, p, velocity=True)
+        assert runs[ve][0][0].steps > 0
+    ref, rc0, vel0 = runs[3]
+    for ve in (2, 6, 7):
+        got, rc, vel = runs[ve]
+        assert rc == rc0
+        for a, b in zip(ref, got):
+            assert a.steps == b.steps and a.converged == b.converged
+            assert np.array_equal(a.q, b.q) and np.array_equal(a.se, b.se), ve
+        assert np.array_equal(vel, vel0), ve
+    assert S.variant_count(prec) == 3 * nv_even
