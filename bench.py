@@ -62,9 +62,20 @@ WORKLOAD = dict(workload="perm-tensor 128^3 prolate-ellipsoid packing (4,4,12) p
 # algorithmic bytes per pore-voxel update: populations read + written once
 # (AA pattern), or for the tau = 1 moment form a 20-byte record read + written
 BYTES_PER_UPDATE = {"fp64": 304, "fp32": 152, "fp16": 76, "bf16": 76, "m32": 40, "m64": 80}
+
+
+def alg_bytes_per_dir_step(prec, npore, nvox):
+    """Algorithmic DRAM bytes of one direction-step: pore-voxel state read and
+    written once plus the bit mask; the dense moment form (md32) reads a
+    20-byte record and a mask byte for every voxel of the box and writes the
+    pore voxels' records."""
+    if prec == "md32":
+        return 20.0 * nvox + 20.0 * npore + 1.0 * nvox
+    return npore * BYTES_PER_UPDATE[prec] + nvox / 8.0
 DTYPE = {"fp16": "f16-storage/f32-compute/f64-reduce", "bf16": "bf16-storage/f32-compute/f64-reduce",
          "fp32": "f32-storage/f32-compute/f64-reduce", "fp64": "f64",
-         "m32": "f32 moment records (tau=1)/f32-compute/f64-reduce", "m64": "f64 moment records (tau=1)"}
+         "m32": "f32 moment records (tau=1)/f32-compute/f64-reduce", "m64": "f64 moment records (tau=1)",
+         "md32": "f32 dense moment records (tau=1)/f32-compute/f64-reduce"}
 # Steps per direction of the converged FP64 solve of the workload structure
 # (x, y, z).  Our FP64 path reproduces the reference's step counts exactly
 # (per-step bit-identical populations; see tests/test_gpu_solve3d.py); the
@@ -139,11 +150,11 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per step launch of the headline kernel from the committed ncu summary."""
-    p = ROOT / "profiles" / "step3d_tensor128.md"
-    if p.exists():
-        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+def profiled_traffic(prec):
+    """DRAM bytes (read + write) per step launch of a path's step kernels, the
+    mean of one odd and one even launch, from the committed ncu summary."""
+    for p in sorted((ROOT / "profiles").glob("*_tensor128.md")):
+        m = re.search(r"traffic_bytes_per_launch\[" + re.escape(prec) + r"\]:\s*([0-9.eE+]+)", p.read_text())
         if m:
             return float(m.group(1))
     return None
@@ -305,10 +316,12 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
         runs_all = []
+        torch.cuda.nvtx.range_push(f"timed:{prec}{':e2e' if host_input else ''}")
         with Clocks(device) as clk, EventTimer(torch, ctx.stream) as t:
             for _ in range(steps):
                 runs, rc, _ = S.solve3d(inp, forces, p, device=device)
                 runs_all.append(runs)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         ms_total = t.ms
         if dist is not None:
@@ -321,7 +334,7 @@ def run_ours(args, rank, world, local_rank):
                     dir_steps=dir_steps, launches=launches)
 
     results = {}
-    cands = [args.precision] if args.precision != "auto" else ["fp32", "fp16", "m32"]
+    cands = [args.precision] if args.precision != "auto" else ["fp32", "fp16", "m32", "md32"]
     if "fp32" not in cands:
         cands.append("fp32")
     for prec in cands:
@@ -345,11 +358,10 @@ def run_ours(args, rank, world, local_rank):
     kt_p, gf_p, ga_p = rates(plain)
     kt_e, _, _ = rates(e2e)
     peak, peak_kind = measured_peak()
-    B = BYTES_PER_UPDATE[head_prec]
-    alg_bytes = head["dir_steps"] * (npore * B + N / 8.0)
+    alg_bytes = head["dir_steps"] * alg_bytes_per_dir_step(head_prec, npore, N)
     achieved = alg_bytes / (head["ms"] / 1e3) / 1e9
     per_launch_alg = alg_bytes / max(1, head["launches"])
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(head_prec)
     serving = serve_trace(device, head_prec, args) if args.serve_seconds > 0 else None
     out = None
     if rank == 0:
@@ -362,7 +374,7 @@ def run_ours(args, rank, world, local_rank):
                          "steps_per_direction": [r.steps for r in m["runs"]],
                          "converged": [r.converged for r in m["runs"]],
                          "rel_err_vs_fp64": m["err"], "kernel_variant": m["variant"],
-                         "hbm_gbs_alg": m["dir_steps"] * (npore * BYTES_PER_UPDATE[p_] + N / 8.0) / (m["ms"] / 1e3) / 1e9}
+                         "hbm_gbs_alg": m["dir_steps"] * alg_bytes_per_dir_step(p_, npore, N) / (m["ms"] / 1e3) / 1e9}
         out = {
             "metric": METRIC, "value": kt, "unit": "k-tensors/hr", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
@@ -492,7 +504,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32", "md32"])
     ap.add_argument("--serve-seconds", type=float, default=5.0)
     ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch"])
     ap.add_argument("--count", type=int, default=32, help="structures of the batch workload")

@@ -23,7 +23,7 @@ WORKLOADS = {
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--workload", default="tensor128", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "fp16", "bf16"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "fp16", "bf16", "m32", "md32"])
     ap.add_argument("--variant", type=int, default=-1, help="step-kernel variant (-1: autotune)")
     ap.add_argument("--steps", type=int, default=24)
     ap.add_argument("--tau", type=float, default=1.0)
