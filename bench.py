@@ -10,7 +10,7 @@ three directions run concurrently on one GPU.
 
 Reported (one JSON line, rank 0):
   value      k-tensors/hour of the headline path, the fastest of FP32
-             populations, FP16 populations and the tau = 1 FP32 moment form that
+             populations, FP16 populations and the tau = 1 FP32 moment forms that
              stays within 1e-3 of the FP64 tensor (every path keeps the
              reference's stopping rule), inputs resident in HBM, device time
              from CUDA events on the solver's stream;
@@ -72,6 +72,8 @@ def alg_bytes_per_dir_step(prec, npore, nvox):
     if prec == "md32":
         return 20.0 * nvox + 20.0 * npore + 1.0 * nvox
     return npore * BYTES_PER_UPDATE[prec] + nvox / 8.0
+
+
 DTYPE = {"fp16": "f16-storage/f32-compute/f64-reduce", "bf16": "bf16-storage/f32-compute/f64-reduce",
          "fp32": "f32-storage/f32-compute/f64-reduce", "fp64": "f64",
          "m32": "f32 moment records (tau=1)/f32-compute/f64-reduce", "m64": "f64 moment records (tau=1)",
@@ -265,9 +267,12 @@ def serve_trace(device, prec, args):
     stats = replay(srv, arrivals, lambda i: (pool[i % len(pool)], forces, p))
     wall = time.perf_counter() - t0
     srv.close()
+    served = stats.completed / wall
     return {"rate_per_s": 20.0, "arrival_seconds": args.serve_seconds, "requests": stats.completed,
             "p50_s": stats.pct(50), "p99_s": stats.pct(99), "max_resident": stats.max_resident,
-            "k_tensors_per_hr": 3600.0 * stats.completed / wall,
+            "p50_queue_s": float(np.percentile(stats.queue_waits, 50)) if stats.queue_waits else None,
+            "k_tensors_per_hr": 3600.0 * served, "served_per_s": served, "overloaded": 20.0 > served,
+            "admission": f"FIFO, HBM budget 150 GiB, resident work cap {srv.max_work} pore-voxel-directions",
             "mix": "batch mix, edges 48 and 64 only (8 seeded structures, reused)", "path": prec}
 
 

@@ -2,9 +2,13 @@
 
 Requests (a structure plus its forcing directions) arrive at any time.  The
 server keeps one resident ``Batch`` (lbm_batch_* in include/lbm.h): between
-CUDA-graph chunks it admits queued requests as long as the HBM budget allows,
-so newly arrived structures join the solves already running on the device,
-and it retires finished ones.  Every result is the same as the structure
+CUDA-graph chunks it admits queued requests in arrival order as long as the
+HBM budget allows and the resident work (pore voxels x directions advanced
+per step) stays under ``max_work``, so newly arrived structures join the
+solves already running on the device, and it retires finished ones.  The work
+cap keeps just enough solves resident to fill the GPU: beyond it, more
+concurrency only slows every resident solve down (all of them finish late
+together) without adding throughput.  Every result is the same as the structure
 solved alone (the batch's flux reduction is independent of the batch's
 contents), and each request's latency is measured from arrival to the end of
 the chunk in which its last direction finished.
@@ -35,6 +39,7 @@ class Request:
     t_admit: float | None = None
     t_done: float | None = None
     results: list | None = None
+    work: int = 0                   # pore voxels x directions
 
 
 @dataclass
@@ -52,8 +57,14 @@ class ServeStats:
 class Server:
     """Continuous-batching solver for one precision and one device."""
 
-    def __init__(self, precision="fp32", hbm_budget=150 * 2**30, chunk=256, device=0, clock=time.perf_counter):
-        self.batch = Batch(precision=precision, hbm_budget=hbm_budget, chunk=chunk, device=device)
+    def __init__(self, precision="fp32", hbm_budget=150 * 2**30, chunk=256, device=0, clock=time.perf_counter,
+                 max_work=2_000_000, batch=None):
+        # `batch` replaces the device batch (an object with the Batch methods
+        # submit/run/poll/resident_bytes/close), for testing the scheduling
+        self.batch = batch if batch is not None else Batch(precision=precision, hbm_budget=hbm_budget,
+                                                           chunk=chunk, device=device)
+        self.max_work = max_work
+        self.resident_work = 0
         self.precision = precision
         self.clock = clock
         self.queue: collections.deque[Request] = collections.deque()
@@ -67,14 +78,17 @@ class Server:
             params = Params3D(**{**params.__dict__, "precision": self.precision})
         rid = self._next
         self._next += 1
-        self.queue.append(Request(rid, np.ascontiguousarray(solid, np.uint8),
-                                  np.asarray(forces, np.float64).reshape(-1, 3), params,
-                                  self.clock() if t_arrive is None else t_arrive))
+        solid = np.ascontiguousarray(solid, np.uint8)
+        forces = np.asarray(forces, np.float64).reshape(-1, 3)
+        self.queue.append(Request(rid, solid, forces, params, self.clock() if t_arrive is None else t_arrive,
+                                  work=int((solid == 0).sum()) * forces.shape[0]))
         return rid
 
     def _admit(self):
         while self.queue:
             r = self.queue[0]
+            if self.inflight and self.max_work and self.resident_work + r.work > self.max_work:
+                break                                     # enough work resident to fill the GPU
             if not self.batch.submit(r.solid, r.forces, r.params, tag=r.rid):
                 if not self.inflight:
                     raise RuntimeError(f"request {r.rid} does not fit the HBM budget even alone")
@@ -82,6 +96,7 @@ class Server:
             self.queue.popleft()
             r.t_admit = self.clock()
             self.inflight[r.rid] = r
+            self.resident_work += r.work
 
     def pump(self, chunks: int = 1):
         """One scheduling round: admit, advance resident solves, retire."""
@@ -92,6 +107,7 @@ class Server:
             t = self.clock()
             for tag, runs in now_done:
                 r = self.inflight.pop(tag)
+                self.resident_work -= r.work
                 r.results, r.t_done = runs, t
                 self.finished[tag] = r
                 self.stats.latencies.append(r.t_done - r.t_arrive)

@@ -146,3 +146,57 @@ def test_poisson_arrivals():
     assert a == poisson_arrivals(20.0, 100.0, seed=1)
     assert all(x < y for x, y in zip(a, a[1:])) and a[-1] < 100.0
     assert 1800 < len(a) < 2200
+
+
+class _FakeBatch:
+    """Stand-in for solver.Batch: a request finishes after `cost` run() calls."""
+
+    def __init__(self, cost=2, budget_slots=1000):
+        self.cost, self.slots = cost, budget_slots
+        self.left = {}
+        self.order = []
+
+    def submit(self, solid, forces, params, tag):
+        if len(self.left) >= self.slots:
+            return False
+        self.left[tag] = self.cost
+        self.order.append(tag)
+        return True
+
+    def run(self, chunks=1):
+        for t in self.left:
+            self.left[t] -= chunks
+
+    def poll(self):
+        done = [t for t, v in self.left.items() if v <= 0]
+        for t in done:
+            del self.left[t]
+        return [(t, ["r"]) for t in done]
+
+    def resident_bytes(self):
+        return 0
+
+    def close(self):
+        pass
+
+
+def test_server_admits_in_order_under_work_cap():
+    """Continuous batching admits in arrival order, keeps the resident work
+    (pore voxels x directions) under the cap, and always admits one request."""
+    from flow_anizotropy_b200.serve import Server
+    from flow_anizotropy_b200.solver import Params3D
+    clock = iter(range(10**6)).__next__
+    fake = _FakeBatch(cost=3)
+    srv = Server(precision="fp32", batch=fake, max_work=3 * 100, clock=lambda: float(clock()))
+    small = np.zeros((4, 5, 5), np.uint8)          # 100 pores
+    big = np.zeros((8, 8, 8), np.uint8)            # 512 pores x 3 > cap: admitted alone
+    forces = [[1e-6, 0, 0]]
+    ids = [srv.submit(s, forces * 3 if s is big else forces, Params3D()) for s in (small, small, big, small)]
+    seen_work = []
+    while not srv.idle():
+        srv.pump()
+        seen_work.append(srv.resident_work)
+        assert srv.resident_work <= 3 * 100 or len(srv.inflight) == 1
+    assert fake.order == ids
+    assert set(srv.results()) == set(ids)
+    assert max(seen_work) > 0
