@@ -268,10 +268,20 @@ def serve_trace(device, prec, args):
     wall = time.perf_counter() - t0
     srv.close()
     served = stats.completed / wall
+    # plain FP32 on the same structures, one tensor at a time (one launch per
+    # step): the baseline the served throughput is compared with
+    pp = Params3D(**{**p.__dict__, "precision": "fp32"})
+    from flow_anizotropy_b200 import solver as S
+    S.solve3d(pool[0], forces, pp, device=device)
+    t0 = time.perf_counter()
+    for s_ in pool:
+        S.solve3d(s_, forces, pp, device=device)
+    plain = len(pool) / (time.perf_counter() - t0)
     return {"rate_per_s": 20.0, "arrival_seconds": args.serve_seconds, "requests": stats.completed,
             "p50_s": stats.pct(50), "p99_s": stats.pct(99), "max_resident": stats.max_resident,
             "p50_queue_s": float(np.percentile(stats.queue_waits, 50)) if stats.queue_waits else None,
             "k_tensors_per_hr": 3600.0 * served, "served_per_s": served, "overloaded": 20.0 > served,
+            "plain_fp32_per_s": plain, "speedup_vs_plain_fp32": served / plain,
             "admission": f"FIFO, HBM budget 150 GiB, resident work cap {srv.max_work} pore-voxel-directions",
             "mix": "batch mix, edges 48 and 64 only (8 seeded structures, reused)", "path": prec}
 
