@@ -235,6 +235,7 @@ __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const
 }
 
 // Block-wide fixed-order sum of three doubles; result valid in thread 0.
+template <int NT = TPB>
 __device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
 {
 #pragma unroll
@@ -246,7 +247,7 @@ __device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
     __syncthreads();
     if (threadIdx.x == 0) {
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        for (int w = 0; w < TPB / 32; ++w) { a0 += sh[w][0]; a1 += sh[w][1]; a2 += sh[w][2]; }
+        for (int w = 0; w < NT / 32; ++w) { a0 += sh[w][0]; a1 += sh[w][1]; a2 += sh[w][2]; }
         v[0] = a0; v[1] = a1; v[2] = a2;
     }
     __syncthreads();
@@ -256,11 +257,12 @@ __device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
 // last tile of the solve to finish sums all partials in a fixed order (the
 // result does not depend on which blocks ran which tiles, or on what else is
 // in the batch) and runs the controller.
+template <int NT = TPB>
 __device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long n,
                                             double (&acc)[3], double (*sh)[3])
 {
     __shared__ int s_last;
-    block_sum3(acc, sh);
+    block_sum3<NT>(acc, sh);
     if (threadIdx.x == 0) {
         double *p = S.partials + 3ll * tile;
         p[0] = acc[0]; p[1] = acc[1]; p[2] = acc[2];
@@ -272,12 +274,12 @@ __device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long
     if (!s_last) return;
     __threadfence();
     double v[3] = {0.0, 0.0, 0.0};
-    for (int t = threadIdx.x; t < S.ntiles; t += TPB) {
+    for (int t = threadIdx.x; t < S.ntiles; t += NT) {
         v[0] += __ldcg(S.partials + 3ll * t);
         v[1] += __ldcg(S.partials + 3ll * t + 1);
         v[2] += __ldcg(S.partials + 3ll * t + 2);
     }
-    block_sum3(v, sh);
+    block_sum3<NT>(v, sh);
     if (threadIdx.x == 0) {
         State3 &st = *S.st;
         st.counter = 0u;

@@ -11,16 +11,18 @@
 //    padded volume with one ghost layer per face holding the periodic image,
 //    so every neighbour of a tile is at a fixed offset and no rank tables are
 //    read; rows are padded to 16 bytes;
-//  * a CTA owns a 32 x 8 column of voxels and marches along z through a
-//    segment of lz planes.  Each z-plane of the column with its halo
+//  * a CTA of 128 threads owns a 32 x 8 column of voxels and marches along z
+//    through a segment of lz planes.  Each z-plane of the column with its halo
 //    (36 x 10 cells x 5 components, plus 48 x 10 mask bytes) arrives by two
 //    TMA tiled loads into a ring of shared-memory slots, completing on an
 //    mbarrier; a plane is loaded once and serves three consecutive output
 //    planes, so global reads are one record per voxel plus halo overlap that
 //    neighbouring CTAs read at the same time (L2 hits);
-//  * the 19-point gather runs out of shared memory (stride-1 across a warp,
-//    no bank conflicts); the new record is stored with coalesced 128-byte
-//    rows, plus the ghost copies of face voxels.
+//  * per plane, one warp compacts the pore cells of the staged mask into a
+//    shared list (ballots), and the threads take pore voxels from the list,
+//    so no lane idles on a solid voxel; the 19-point gather runs out of shared
+//    memory; the new record is stored with row-ordered (mostly coalesced)
+//    stores, plus the ghost copies of face voxels.
 //
 // Global traffic per voxel-step: 20 B read (every voxel) + 20 B written (pore
 // voxels) + 1 B of mask, against 152 B per pore voxel for FP32 populations.
@@ -34,8 +36,10 @@
 
 namespace lbm {
 
-constexpr int MD_BX = 32;                                   // tile width (x): one warp
-constexpr int MD_BY = TPB / 32;                             // tile height (y): one row per warp
+constexpr int MD_TPB = 128;                                 // threads per CTA
+constexpr int MD_BX = 32;                                   // tile width (x)
+constexpr int MD_BY = 8;                                    // tile height (y)
+constexpr int MD_CELLS = MD_BX * MD_BY;                     // voxels of a tile plane
 constexpr int MD_HX = 36;                                   // record box width: x0-1 .. x0+34 (144 B)
 constexpr int MD_HY = MD_BY + 2;
 constexpr int MD_MX = 48;                                   // mask box width (48 B)
@@ -52,7 +56,7 @@ constexpr int MD_STATUS_TIMEOUT = 5;
 
 // ring depth and register budget per variant (z-segment length: md_lz)
 __host__ __device__ constexpr int md_ns(int v) { return v == 3 ? 6 : 4; }
-__host__ __device__ constexpr int md_minb(int v) { return v == 3 ? 3 : 4; }
+__host__ __device__ constexpr int md_minb(int v) { return v == 3 ? 5 : 7; }
 inline size_t md_smem_bytes(int v) { return (size_t)md_ns(v) * MD_SLOT + 128; }
 
 inline long long md_lattice_bytes(const MDGeom &g) { return MD_MAPS_BYTES + 2ll * MD_NC * g.vol * 4; }
@@ -145,13 +149,15 @@ struct MDGather<Q3> {
 };
 
 template <int NS, int MINB>
-__global__ void __launch_bounds__(TPB, MINB) stepmd_kernel(const StepArgs a)
+__global__ void __launch_bounds__(MD_TPB, MINB) stepmd_kernel(const StepArgs a)
 {
     extern __shared__ unsigned char md_raw[];
     __shared__ uint64_t bars[NS];
-    __shared__ double sh[TPB / 32][3];
+    __shared__ double sh[MD_TPB / 32][3];
+    __shared__ unsigned char list[MD_CELLS];                // pore cells of the current plane
+    __shared__ int list_n;
     unsigned char *sm = md_raw + ((128u - (smem_u32(md_raw) & 127u)) & 127u);
-    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
         mbar_init_fence();
@@ -175,8 +181,6 @@ __global__ void __launch_bounds__(TPB, MINB) stepmd_kernel(const StepArgs a)
         const int zs = (t / G.nyt) * G.lz;
         const int ze = min(zs + G.lz, S.nz);
         const int x0 = txi * MD_BX, y0 = tyi * MD_BY;
-        const int x = x0 + tx, y = y0 + ty;
-        const bool inxy = x < S.nx && y < S.ny;
         char *lat = static_cast<char *>(S.A);
         float *dst = reinterpret_cast<float *>(lat + MD_MAPS_BYTES) + (n & 1ll) * (MD_NC * G.vol);
         const float Fx = (float)S.P.F[0], Fy = (float)S.P.F[1], Fz = (float)S.P.F[2];
@@ -184,8 +188,10 @@ __global__ void __launch_bounds__(TPB, MINB) stepmd_kernel(const StepArgs a)
         double acc3[3] = {0.0, 0.0, 0.0};
         if (n == 1) {
             // moments of the initial state f = w: rho = 1, j = 0
-            if (inxy)
-                for (int z = zs; z < ze; ++z) {
+            for (int z = zs; z < ze; ++z)
+                for (int cell = tid; cell < MD_CELLS; cell += MD_TPB) {
+                    const int x = x0 + (cell & (MD_BX - 1)), y = y0 + cell / MD_BX;
+                    if (x >= S.nx || y >= S.ny) continue;
                     if (mbit(S.mask + ((size_t)z * S.ny + y) * S.wpr, x)) continue;
                     const float ux = 0.5f * Fx, uy = 0.5f * Fy, uz = 0.5f * Fz;
                     float c1n, d3n;
@@ -213,8 +219,7 @@ __global__ void __launch_bounds__(TPB, MINB) stepmd_kernel(const StepArgs a)
             }
             int waited = 0;
             bool bad = false;
-            const int c = (ty + 1) * MD_HX + (tx + 1);
-            const int cm = (ty + 1) * MD_MX + (tx + 1);
+            const int xlim = S.nx - x0, ylim = S.ny - y0;   // valid cells: tx < xlim, ty < ylim
             for (int z = zs; z < ze; ++z) {
                 const int j = z - zs + 1;                    // slot index of plane z
                 while (waited <= j + 1) {
@@ -229,30 +234,45 @@ __global__ void __launch_bounds__(TPB, MINB) stepmd_kernel(const StepArgs a)
                     }
                     ++waited;
                 }
-                if (!bad && inxy) {
-                    const float *R[3] = {reinterpret_cast<const float *>(sm + ((j - 1) % NS) * MD_SLOT),
-                                         reinterpret_cast<const float *>(sm + (j % NS) * MD_SLOT),
-                                         reinterpret_cast<const float *>(sm + ((j + 1) % NS) * MD_SLOT)};
-                    const uint8_t *M[3] = {sm + ((j - 1) % NS) * MD_SLOT + MD_MASK_OFF,
-                                           sm + (j % NS) * MD_SLOT + MD_MASK_OFF,
-                                           sm + ((j + 1) % NS) * MD_SLOT + MD_MASK_OFF};
-                    if (!M[1][cm]) {
-                        const float *own = R[1] + c;
-                        float acc[4] = {pop_rec<0, float>(own[0], own[4 * MD_PLANE], own[MD_PLANE],
-                                                          own[2 * MD_PLANE], own[3 * MD_PLANE], 1.0f, pr, Fx, Fy,
-                                                          Fz),
-                                        0.0f, 0.0f, 0.0f};
-                        MDGather<1>::run(R, M, c, cm, own, pr, Fx, Fy, Fz, acc);
-                        const float dr = acc[0];
-                        const float rho = 1.0f + dr;
-                        const float ux = (acc[1] + 0.5f * Fx) / rho;
-                        const float uy = (acc[2] + 0.5f * Fy) / rho;
-                        const float uz = (acc[3] + 0.5f * Fz) / rho;
-                        float c1n, d3n;
-                        make_record<float>(dr, ux, uy, uz, Fx, Fy, Fz, pr, c1n, d3n);
-                        md_store(dst, S, x, y, z, c1n, ux, uy, uz, d3n);
-                        acc3[0] += (double)ux; acc3[1] += (double)uy; acc3[2] += (double)uz;
+                const float *R[3] = {reinterpret_cast<const float *>(sm + ((j - 1) % NS) * MD_SLOT),
+                                     reinterpret_cast<const float *>(sm + (j % NS) * MD_SLOT),
+                                     reinterpret_cast<const float *>(sm + ((j + 1) % NS) * MD_SLOT)};
+                const uint8_t *M[3] = {sm + ((j - 1) % NS) * MD_SLOT + MD_MASK_OFF,
+                                       sm + (j % NS) * MD_SLOT + MD_MASK_OFF,
+                                       sm + ((j + 1) % NS) * MD_SLOT + MD_MASK_OFF};
+                // warp 0 compacts the pore cells of plane z, row by row
+                if (tid < 32) {
+                    int cnt = 0;
+#pragma unroll
+                    for (int r = 0; r < MD_BY; ++r) {
+                        const bool pore = lane < xlim && r < ylim && !M[1][(r + 1) * MD_MX + lane + 1];
+                        const unsigned b = __ballot_sync(0xffffffffu, pore);
+                        if (pore) list[cnt + __popc(b & ((1u << lane) - 1u))] = (unsigned char)(r * MD_BX + lane);
+                        cnt += __popc(b);
                     }
+                    if (lane == 0) list_n = cnt;
+                }
+                __syncthreads();
+                const int npz = bad ? 0 : list_n;
+                for (int q = tid; q < npz; q += MD_TPB) {
+                    const int cell = list[q];
+                    const int tx = cell & (MD_BX - 1), ty = cell / MD_BX;
+                    const int c = (ty + 1) * MD_HX + (tx + 1);
+                    const int cm = (ty + 1) * MD_MX + (tx + 1);
+                    const float *own = R[1] + c;
+                    float acc[4] = {pop_rec<0, float>(own[0], own[4 * MD_PLANE], own[MD_PLANE], own[2 * MD_PLANE],
+                                                      own[3 * MD_PLANE], 1.0f, pr, Fx, Fy, Fz),
+                                    0.0f, 0.0f, 0.0f};
+                    MDGather<1>::run(R, M, c, cm, own, pr, Fx, Fy, Fz, acc);
+                    const float dr = acc[0];
+                    const float rho = 1.0f + dr;
+                    const float ux = (acc[1] + 0.5f * Fx) / rho;
+                    const float uy = (acc[2] + 0.5f * Fy) / rho;
+                    const float uz = (acc[3] + 0.5f * Fz) / rho;
+                    float c1n, d3n;
+                    make_record<float>(dr, ux, uy, uz, Fx, Fy, Fz, pr, c1n, d3n);
+                    md_store(dst, S, x0 + tx, y0 + ty, z, c1n, ux, uy, uz, d3n);
+                    acc3[0] += (double)ux; acc3[1] += (double)uy; acc3[2] += (double)uz;
                 }
                 if (__syncthreads_or(bad)) {
                     if (tid == 0) {
@@ -267,7 +287,7 @@ __global__ void __launch_bounds__(TPB, MINB) stepmd_kernel(const StepArgs a)
                 if (tid == 0 && j - 1 + NS < np) issue(j - 1 + NS);
             }
         }
-        if (red) finish_tile(S, item.y, n, acc3, sh);
+        if (red) finish_tile<MD_TPB>(S, item.y, n, acc3, sh);
     }
 }
 

@@ -83,10 +83,10 @@ cudaError_t launch_stepmd(int v, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
     const size_t smem = md_smem_bytes(v);
     switch (v) {
-    case 0: LBM_MD(0)<<<grid, TPB, smem, s>>>(a); break;
-    case 1: LBM_MD(1)<<<grid, TPB, smem, s>>>(a); break;
-    case 2: LBM_MD(2)<<<grid, TPB, smem, s>>>(a); break;
-    case 3: LBM_MD(3)<<<grid, TPB, smem, s>>>(a); break;
+    case 0: LBM_MD(0)<<<grid, MD_TPB, smem, s>>>(a); break;
+    case 1: LBM_MD(1)<<<grid, MD_TPB, smem, s>>>(a); break;
+    case 2: LBM_MD(2)<<<grid, MD_TPB, smem, s>>>(a); break;
+    case 3: LBM_MD(3)<<<grid, MD_TPB, smem, s>>>(a); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -96,7 +96,7 @@ int max_blocks_stepmd(int v)
 {
     const void *k = md_kernel(v);
     int nb = 0;
-    if (k) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, md_smem_bytes(v));
+    if (k) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, MD_TPB, md_smem_bytes(v));
     return nb;
 }
 
