@@ -115,7 +115,7 @@ def parse(argv):
             sys.stderr.write(USAGE)
             raise Die("unknown option " + a)
         i += 1
-    if cfg["precision"] not in ("fp64", "fp32", "fp16", "bf16"):
+    if cfg["precision"] not in ("fp64", "fp32", "fp16", "bf16", "m32", "m64", "md32"):
         raise Die("unknown precision " + cfg["precision"])
     if cfg["criterion"] not in ("drift", "block", "auto"):
         raise Die("unknown criterion " + cfg["criterion"])

@@ -26,7 +26,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .solver import Batch, Params3D
+from .solver import Batch, LBMError, Params3D
 
 
 @dataclass
@@ -40,6 +40,7 @@ class Request:
     t_done: float | None = None
     results: list | None = None
     work: int = 0                   # pore voxels x directions
+    error: str | None = None        # set when the request was rejected (bad input)
 
 
 @dataclass
@@ -89,7 +90,16 @@ class Server:
             r = self.queue[0]
             if self.inflight and self.max_work and self.resident_work + r.work > self.max_work:
                 break                                     # enough work resident to fill the GPU
-            if not self.batch.submit(r.solid, r.forces, r.params, tag=r.rid):
+            try:
+                admitted = self.batch.submit(r.solid, r.forces, r.params, tag=r.rid)
+            except LBMError as e:
+                # this request's input is bad (e.g. no pore space): report it
+                # as finished with an error and go on with the queue
+                self.queue.popleft()
+                r.error, r.t_done = str(e), self.clock()
+                self.finished[r.rid] = r
+                continue
+            if not admitted:
                 if not self.inflight:
                     raise RuntimeError(f"request {r.rid} does not fit the HBM budget even alone")
                 break                                     # wait for retirements

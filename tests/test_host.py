@@ -1,5 +1,6 @@
 """Host-side logic without a GPU: structure I/O, CLI argument handling,
 tensor algebra, generators, and the C ABI's exported symbols."""
+import os
 import re
 import subprocess
 import sys
@@ -200,3 +201,50 @@ def test_server_admits_in_order_under_work_cap():
     assert fake.order == ids
     assert set(srv.results()) == set(ids)
     assert max(seen_work) > 0
+
+
+def _dataset(tmp_path, shapes, seed=0):
+    """A structures.csv dataset in the layout of the reference generator."""
+    import pandas as pd
+    from flow_anizotropy_b200 import structures as st
+    from flow_anizotropy_b200.structure_io3d import save_structure
+    d = tmp_path / "ds"
+    (d / "structures").mkdir(parents=True)
+    rows = []
+    for i, shp in enumerate(shapes):
+        solid = st.sphere_packing(shp, 3.0, 0.6, seed=seed + i, percolate=(True, True, True))
+        name = f"s{i:04d}.raw"
+        save_structure(d / "structures" / name, solid)
+        rows.append({"sample_id": i, "filename": name, "group": "ab"[i % 2]})
+    pd.DataFrame(rows).to_csv(d / "structures.csv", index=False)
+    return d
+
+
+def test_batch3d_plan_resume_and_atomic_rows(tmp_path):
+    """Task planning (limit, shard, interleave), the resume rule (complete CSVs
+    cached, incomplete ones removed and redone) and the atomic row write."""
+    from flow_anizotropy_b200 import batch3d as B
+    from flow_anizotropy_b200.solver import Result3D
+    d = _dataset(tmp_path, [(10, 11, 12)] * 5)
+    tasks = B.plan(str(d))
+    assert [t.sample_id for t in tasks] == [0, 1, 2, 3, 4]
+    assert tasks[0].structure == str(d / "structures" / "s0000.raw")
+    assert tasks[0].out_csv == str(d / "perm" / "000000.csv")
+    assert [t.sample_id for t in B.plan(str(d), shard="1/2")] == [1, 3]
+    assert [t.sample_id for t in B.plan(str(d), limit=3)] == [0, 1, 2]
+    assert [t.sample_id for t in B.plan(str(d), interleave="group")] == [0, 1, 2, 3, 4]
+    cfg = B.solver_config("--eps 1e-6 --lag 500 --validate", "fp32")
+    assert cfg["eps"] == 1e-6 and cfg["lag"] == 500 and cfg["validate"] and cfg["precision"] == "fp32"
+    cfg["ff"] = 1.0
+    (d / "perm").mkdir()
+    solid = np.zeros((12, 11, 10), np.uint8)
+    runs = [Result3D(q=np.array([1e-6 if c == j else 1e-9 for c in range(3)]), se=np.zeros(3), steps=5000,
+                     converged=int(j != 2), status=0) for j in range(3)]
+    assert B.write_row(tasks[0], cfg, solid, runs) == 3           # a direction did not converge
+    assert B.valid_result(tasks[0].out_csv)
+    assert not any(".tmp." in f for f in os.listdir(d / "perm"))
+    Path(tasks[1].out_csv).write_text("filename,K_xx\n")         # left by a killed run
+    work, cached = B.todo(tasks)
+    assert [t.sample_id for t in cached] == [0]
+    assert [t.sample_id for t in work] == [1, 2, 3, 4]
+    assert not Path(tasks[1].out_csv).exists()
