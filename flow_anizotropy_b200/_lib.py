@@ -27,6 +27,7 @@ SYMBOLS = (
     "lbm_batch_run", "lbm_batch_poll", "lbm_batch_active", "lbm_batch_resident_bytes",
     "lbm_variant_count", "lbm_tune3d",
     "lbm_debug_steps3d", "lbm_debug_steps2d",
+    "lbm_trig_structure3d", "lbm_percolates3d",
 )
 
 
@@ -127,6 +128,11 @@ def load(path: Path | str | None = None):
         L.lbm_debug_steps2d.argtypes = [vp, u8p, C.c_int, C.c_int, dp, C.c_double,
                                         C.c_longlong, fp, fp, dp]
         L.lbm_debug_steps2d.restype = C.c_int
+        ip = C.POINTER(C.c_int32)
+        L.lbm_trig_structure3d.argtypes = [vp, C.c_int, C.c_int, ip, dp, dp, C.c_double, C.c_double, u8p, dp]
+        L.lbm_trig_structure3d.restype = C.c_int
+        L.lbm_percolates3d.argtypes = [vp, u8p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]
+        L.lbm_percolates3d.restype = C.c_int
         _lib = L
         return L
 

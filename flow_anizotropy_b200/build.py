@@ -34,6 +34,7 @@ UNITS = {
     "engine2.cu": [],
     "engine2_noalloc.cu": [],
     "engine_batch.cu": [],
+    "gen3d.cu": ["-fmad=false"],
 }
 
 

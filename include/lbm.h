@@ -203,6 +203,23 @@ int  lbm_batch_poll(lbm_batch *batch, long long *tags, int *dirs,
 int       lbm_batch_active(const lbm_batch *batch);
 long long lbm_batch_resident_bytes(const lbm_batch *batch);
 
+/* ---- structure generation (scripts/gen_aniso_structures3d.py datasets) - */
+
+/* The random trigonometric field of gen_aniso_structures3d.py:154-176 over a
+ * size^3 periodic cell, S = scale * sum_m cos(((2 pi qz_m) z + (2 pi qy_m) y)
+ * + (2 pi qx_m) x + phases[m]) at the coordinates pts[0..size) of each axis,
+ * in the reference's operation order; *threshold = numpy's linear quantile of
+ * S at `porosity` (:179-181) and solid_out = S > *threshold (size^3 bytes,
+ * x fastest; host or device pointer).  q: n_modes x 3 int32 (qx, qy, qz). */
+int lbm_trig_structure3d(lbm_ctx *ctx, int size, int n_modes, const int32_t *q, const double *phases,
+                         const double *pts, double scale, double porosity, uint8_t *solid_out,
+                         double *threshold);
+
+/* Percolation of the pore phase (solid = 0) of gen_aniso_structures3d.py:184-205:
+ * 6-connected components of the 3 x 3 x 3 tiling; perc[a] = 1 if a component
+ * touches both faces of axis a (x, y, z).  27 nx ny nz < 2^31. */
+int lbm_percolates3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz, int perc[3]);
+
 /* ---- autotuning ------------------------------------------------------ */
 
 /* Number of step-kernel variants (pore voxels per thread x register budget)
