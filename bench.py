@@ -485,6 +485,37 @@ def run_batch_workload(args, device=0):
     return out
 
 
+def run_gen_workload(args, device=0):
+    """Structure generation (the gen_aniso_structures3d.py dataset model,
+    default knobs) at --gen-size: samples/s of the device generator against
+    the CPU restatement of the reference's per-voxel work (numpy field and
+    quantile, scipy labelling of the 3x3x3 tiling) on one host core, on the
+    same samples; the structures are checked to be identical."""
+    import torch
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200 import gen3d as G
+    from oracle import gen3d_oracle as GO
+    n = args.count
+    gen = G.Generator(size=args.gen_size)
+    gen.sample(0)                                        # warm-up
+    ctx = _lib.context(device)
+    with EventTimer(torch, ctx.stream) as t:
+        t0 = time.perf_counter()
+        got = [gen.sample(i) for i in range(1, n + 1)]
+        wall = time.perf_counter() - t0
+    attempts = sum(r[1]["attempts"] for r in got if r is not None)
+    cpu_n = max(1, min(n, 3))
+    t0 = time.perf_counter()
+    ref = [GO.sample(i, args.gen_size) for i in range(1, cpu_n + 1)]
+    cpu = time.perf_counter() - t0
+    same = all(np.array_equal(a[0], b[0]) for a, b in zip(got[:cpu_n], ref) if a is not None and b is not None)
+    return {"workload": f"gen_aniso_structures3d model, {args.gen_size}^3, default knobs, {n} samples",
+            "samples_per_s": n / wall, "attempts": attempts, "device_ms": t.ms,
+            "cpu_baseline": {"samples_per_s": cpu_n / cpu, "cores": 1, "kind": "port",
+                             "sample": f"{cpu_n} samples, numpy field + quantile, scipy labelling"},
+            "speedup_vs_cpu_core": (n / wall) / (cpu_n / cpu), "identical_structures": same}
+
+
 # -------------------------------------------------------- reference arm ----
 def run_reference(args, rank, world):
     if rank != 0:
@@ -521,7 +552,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32", "md32"])
     ap.add_argument("--serve-seconds", type=float, default=5.0)
-    ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch"])
+    ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch", "gen3d"])
+    ap.add_argument("--gen-size", type=int, default=80, help="cell edge of the gen3d workload")
     ap.add_argument("--count", type=int, default=32, help="structures of the batch workload")
     ap.add_argument("--batch-paths", default="fp32,m32,fp16")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -533,6 +565,8 @@ def main():
         out = run_reference(args, rank, world)
     elif args.workload == "batch":
         out = run_batch_workload(args, local_rank) if rank == 0 else None
+    elif args.workload == "gen3d":
+        out = run_gen_workload(args, local_rank) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None and rank == 0:
