@@ -485,6 +485,42 @@ def run_batch_workload(args, device=0):
     return out
 
 
+def run_large_workload(args, device=0):
+    """The large configuration: 512^3 Gaussian random field (sigma (3, 3, 9),
+    phi = 0.15, largest cluster spanning z), tau = 0.8, three directions
+    resident; a fixed number of steps (--large-steps) per storage precision,
+    timed with CUDA events after the autotuner's pick: fluid GLUPS and the
+    HBM roofline of the step kernels (a converged tensor at this size takes
+    tens of thousands of steps, beyond a bench run)."""
+    import torch
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200 import solver as S
+    from flow_anizotropy_b200 import structures as st
+    solid = st.large_grf(0, n=args.large_n)
+    npore, N = int((solid == 0).sum()), solid.size
+    dev = torch.from_numpy(np.ascontiguousarray(solid)).cuda(device)
+    ctx = _lib.context(device)
+    F = 1e-6
+    forces = [[F, 0, 0], [0, F, 0], [0, 0, F]]
+    peak, peak_kind = measured_peak()
+    out = {"workload": f"{args.large_n}^3 GRF sigma (3,3,9) phi=0.15 largest z-spanning cluster, tau 0.8, 3 directions",
+           "pore_voxels": npore, "voxels": N, "steps": args.large_steps, "paths": {}}
+    for prec in ("fp32", "fp16"):
+        best, _ = S.tune3d(solid, ndir=3, precision=prec, nsteps=50, device=device)
+        p = S.Params3D(tau=0.8, eps=0.0, lag=10**9, hold=10**6, min_steps=0, max_steps=args.large_steps,
+                       avg_steps=0, precision=prec, criterion="drift", variant=best)
+        S.solve3d(dev, forces, S.Params3D(**{**p.__dict__, "max_steps": 20}), device=device)
+        with Clocks(device) as clk, EventTimer(torch, ctx.stream) as t:
+            runs, _, _ = S.solve3d(dev, forces, p, device=device)
+        upd = 3.0 * npore * args.large_steps
+        ab = 3.0 * args.large_steps * alg_bytes_per_dir_step(prec, npore, N)
+        out["paths"][prec] = {"ms": t.ms, "glups_fluid": upd / (t.ms / 1e3) / 1e9, "kernel_variant": best,
+                              "roofline": {"achieved": ab / (t.ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                           "frac": ab / (t.ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+                              "clocks": clk.summary()}
+    return out
+
+
 def run_gen_workload(args, device=0):
     """Structure generation (the gen_aniso_structures3d.py dataset model,
     default knobs) at --gen-size: samples/s of the device generator against
@@ -552,7 +588,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32", "md32"])
     ap.add_argument("--serve-seconds", type=float, default=5.0)
-    ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch", "gen3d"])
+    ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch", "gen3d", "large"])
+    ap.add_argument("--large-n", type=int, default=512, help="cell edge of the large workload")
+    ap.add_argument("--large-steps", type=int, default=2000)
     ap.add_argument("--gen-size", type=int, default=80, help="cell edge of the gen3d workload")
     ap.add_argument("--count", type=int, default=32, help="structures of the batch workload")
     ap.add_argument("--batch-paths", default="fp32,m32,fp16")
@@ -567,6 +605,8 @@ def main():
         out = run_batch_workload(args, local_rank) if rank == 0 else None
     elif args.workload == "gen3d":
         out = run_gen_workload(args, local_rank) if rank == 0 else None
+    elif args.workload == "large":
+        out = run_large_workload(args, local_rank) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None and rank == 0:
