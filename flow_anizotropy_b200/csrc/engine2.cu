@@ -54,13 +54,27 @@ void init_state2(State2 &st, const Ctl2 &c)
     }
 }
 
+// The host loop of LMB2d/main.cpp:99-235 with the controller on the device:
+// launch up to the next step at which some direction's controller can change
+// phase, then read the states back.  The launches in between are replayed
+// from a CUDA graph of kGraphSteps step launches (plus the s_base advance),
+// which removes most of the per-launch overhead of this small, launch-bound
+// lattice; the step numbers and kernels are the same as single launches.
+constexpr int kGraphSteps = 100;
+
 static int run_plain2d(lbm_ctx *ctx, std::vector<Solve2> &hs, Solve2 *d_solves, State2 *d_states,
                        const int2 *d_work, int nwork, std::vector<State2> &hst)
 {
     const int n = (int)hs.size();
-    long long s = 0;
+    long long s = 0, base = 0;        // steps done; s_base of every solve (host copy)
     StepArgs2 a;
     a.solves = d_solves; a.work = d_work; a.nwork = nwork;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    struct GraphGuard {
+        cudaGraph_t &g; cudaGraphExec_t &e;
+        ~GraphGuard() { if (e) cudaGraphExecDestroy(e); if (g) cudaGraphDestroy(g); }
+    } guard{graph, exec};
     for (;;) {
         CK(cudaMemcpyAsync(hst.data(), d_states, sizeof(State2) * n, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -77,9 +91,30 @@ static int run_plain2d(lbm_ctx *ctx, std::vector<Solve2> &hs, Solve2 *d_solves, 
             }
         }
         if (target == LLONG_MAX) break;
-        for (; s < target; ++s) {
-            a.step = s;
-            CK(launch_step2d(dim3(nwork), ctx->stream, a));
+        if (!exec && target - s >= kGraphSteps) {
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = cudaSuccess;
+            for (int i = 0; i < kGraphSteps && e == cudaSuccess; ++i) {
+                StepArgs2 g = a;
+                g.step = i;
+                e = launch_step2d(dim3(nwork), ctx->stream, g);
+            }
+            if (e == cudaSuccess) e = launch_advance2d(d_solves, n, kGraphSteps, ctx->stream);
+            const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
+            CK(e);
+            CK(e2);
+            CK(cudaGraphInstantiate(&exec, graph, 0));
+        }
+        while (s < target) {
+            if (exec && target - s >= kGraphSteps) {
+                CK(cudaGraphLaunch(exec, ctx->stream));
+                s += kGraphSteps;
+                base += kGraphSteps;
+            } else {
+                a.step = s - base;
+                CK(launch_step2d(dim3(nwork), ctx->stream, a));
+                ++s;
+            }
         }
     }
     return LBM_OK;

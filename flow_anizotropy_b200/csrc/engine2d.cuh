@@ -244,5 +244,6 @@ __global__ void canon2d_kernel(const Solve2 S, long long done, float *f_out);
 __global__ void fieldres2d_kernel(const float *snap, const float *last, int nn, double *out);
 
 cudaError_t launch_step2d(dim3 grid, cudaStream_t s, const StepArgs2 &a);
+cudaError_t launch_advance2d(const Solve2 *solves, int nsolves, long long steps, cudaStream_t s);
 
 }  // namespace lbm

@@ -124,6 +124,20 @@ __global__ void fieldres2d_kernel(const float *snap, const float *last, int nn, 
     if (threadIdx.x == 0) { atomicAdd(out, v[0]); atomicAdd(out + 1, v[1]); }
 }
 
+// s_base += steps for every solve of a launch list (the step numbers of a
+// replayed chunk of step launches are relative to s_base)
+__global__ void advance2d_kernel(const Solve2 *solves, int nsolves, long long steps)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < nsolves) solves[j].st->s_base += steps;
+}
+
+cudaError_t launch_advance2d(const Solve2 *solves, int nsolves, long long steps, cudaStream_t s)
+{
+    advance2d_kernel<<<(nsolves + 127) / 128, 128, 0, s>>>(solves, nsolves, steps);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_step2d(dim3 grid, cudaStream_t s, const StepArgs2 &a)
 {
     step2d_kernel<<<grid, TPB, 0, s>>>(a);
