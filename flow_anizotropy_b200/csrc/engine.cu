@@ -361,7 +361,13 @@ void lbm_copy_pores(Solve3 &dst, const Solve3 &src)
 
 // Run a set of 3D solves sharing one mask to completion, one launch per step.
 // The host synchronises only where the controller can change phase: on lag
-// multiples and max_steps in phase 1, at the end of the averaging phase.
+// multiples and max_steps in phase 1, at the end of the averaging phase.  In
+// between, whole chunks of kGraphSteps3 launches (an even count, starting on
+// an even step, plus the s_base advance) are replayed from a CUDA graph, which
+// removes the per-launch overhead that dominates small structures; the step
+// numbers and kernels are those of single launches.
+constexpr int kGraphSteps3 = 64;
+
 static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, State3 *d_states,
                        const int2 *d_work, int nwork, int prec, int variant, std::vector<State3> &hst)
 {
@@ -369,7 +375,7 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
     bool w1 = true;
     for (const Solve3 &S : hs) w1 = w1 && S.P.tau == 1.0;
     variant = lbm_effective_variant(prec, variant, hs.empty() || hs[0].meta != nullptr);
-    long long s = 0;
+    long long s = 0, base = 0;        // steps done; s_base of the unfinished solves (host copy)
     StepArgs a;
     a.solves = d_solves; a.work = d_work; a.nwork_dev = nullptr; a.nwork = nwork;
     StepArgs ae = a;                  // even steps (grouped work list for grouped variants)
@@ -383,6 +389,17 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
         ae.work = static_cast<const int2 *>(gwork.p);
         ae.nwork = (int)items.size();
     }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    struct GraphGuard {
+        cudaGraph_t &g; cudaGraphExec_t &e;
+        ~GraphGuard() { if (e) cudaGraphExecDestroy(e); if (g) cudaGraphDestroy(g); }
+    } guard{graph, exec};
+    auto launch = [&](long long rel, bool odd) {
+        StepArgs x = odd ? a : ae;
+        x.step = rel;
+        return lbm_launch_step(prec, variant, w1, odd, dim3(x.nwork), ctx->stream, x);
+    };
     for (;;) {
         CK(cudaMemcpyAsync(hst.data(), d_states, sizeof(State3) * n, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -399,12 +416,36 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
             }
         }
         if (target == LLONG_MAX) break;
-        for (; s < target; ++s) {
-            // every solve of the call is at step s + 1 (they start together)
-            const bool odd = ((s + 1) & 1) == 1;
-            StepArgs &x = odd ? a : ae;
-            x.step = s;
-            CK(lbm_launch_step(prec, variant, w1, odd, dim3(x.nwork), ctx->stream, x));
+        if (!exec && target - s >= 2 * kGraphSteps3) {
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = cudaSuccess;
+            // launch i of a chunk runs step i + 1 after s_base (s_base even)
+            for (int i = 0; i < kGraphSteps3 && e == cudaSuccess; ++i) e = launch(i, ((i + 1) & 1) == 1);
+            if (e == cudaSuccess) {
+                advance3d_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(d_solves, n, kGraphSteps3);
+                e = cudaGetLastError();
+            }
+            const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
+            CK(e);
+            CK(e2);
+            CK(cudaGraphInstantiate(&exec, graph, 0));
+        }
+        while (s < target) {
+            if (exec && (s & 1) == 0 && target - s >= kGraphSteps3) {
+                if (base != s) {
+                    // a chunk numbers its steps from s_base: catch up with the single steps
+                    advance3d_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(d_solves, n, s - base);
+                    CK(cudaGetLastError());
+                    base = s;
+                }
+                CK(cudaGraphLaunch(exec, ctx->stream));
+                s += kGraphSteps3;
+                base += kGraphSteps3;
+            } else {
+                // every unfinished solve of the call is at step s + 1 (they start together)
+                CK(launch(s - base, ((s + 1) & 1) == 1));
+                ++s;
+            }
         }
     }
     return LBM_OK;

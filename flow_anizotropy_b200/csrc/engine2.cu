@@ -107,6 +107,11 @@ static int run_plain2d(lbm_ctx *ctx, std::vector<Solve2> &hs, Solve2 *d_solves, 
         }
         while (s < target) {
             if (exec && target - s >= kGraphSteps) {
+                if (base != s) {
+                    // a chunk numbers its steps from s_base: catch up with the single steps
+                    CK(launch_advance2d(d_solves, n, s - base, ctx->stream));
+                    base = s;
+                }
                 CK(cudaGraphLaunch(exec, ctx->stream));
                 s += kGraphSteps;
                 base += kGraphSteps;

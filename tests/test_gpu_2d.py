@@ -30,10 +30,15 @@ def test_bitwise_steps(gpu, shape, nsteps):
     np.testing.assert_allclose(q, o.q(), rtol=1e-14, atol=1e-30)
 
 
-def test_solve_matches_oracle(gpu):
+@pytest.mark.parametrize("prm", [
+    dict(eps=1e-3, lag=500, hold=3, min_steps=1000, max_steps=4000, avg_steps=500, avg_sample=50),
+    # lag and averaging lengths that are not multiples of the solve loop's
+    # replayed chunk, so chunks and single launches interleave
+    dict(eps=1e-3, lag=250, hold=3, min_steps=550, max_steps=3000, avg_steps=350, avg_sample=25),
+])
+def test_solve_matches_oracle(gpu, prm):
     solid = _solid((64, 64), 3, 0.25)
     F = 2.5e-7
-    prm = dict(eps=1e-3, lag=500, hold=3, min_steps=1000, max_steps=4000, avg_steps=500, avg_sample=50)
     runs, rc, vel = S.solve2d(solid, [[F, 0], [0, F]], S.Params2D(**prm), velocity=True)
     for j, f in enumerate(([F, 0], [0, F])):
         r = O.solve2d(solid, f, velocity=True, **prm)
