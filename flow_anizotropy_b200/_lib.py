@@ -22,7 +22,7 @@ CRIT_DRIFT, CRIT_BLOCK = 0, 1
 # Exported symbols, exactly those include/lbm.h declares.
 SYMBOLS = (
     "lbm_version", "lbm_create", "lbm_destroy", "lbm_last_error", "lbm_stream",
-    "lbm_solve3d", "lbm_solve2d", "lbm_solve2d_noalloc",
+    "lbm_solve3d", "lbm_solve2d", "lbm_solve2d_many", "lbm_solve2d_noalloc",
     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_bytes3d", "lbm_batch_submit3d",
     "lbm_batch_run", "lbm_batch_poll", "lbm_batch_active", "lbm_batch_resident_bytes",
     "lbm_variant_count", "lbm_tune3d",
@@ -97,6 +97,9 @@ def load(path: Path | str | None = None):
         L.lbm_solve2d.argtypes = [vp, u8p, C.c_int, C.c_int, C.c_int, dp,
                                   C.POINTER(Params2D), C.POINTER(Result2D), fp]
         L.lbm_solve2d.restype = C.c_int
+        L.lbm_solve2d_many.argtypes = [vp, C.c_int, u8p, C.c_int, C.c_int, C.c_int, dp,
+                                       C.POINTER(Params2D), C.POINTER(Result2D)]
+        L.lbm_solve2d_many.restype = C.c_int
         L.lbm_solve2d_noalloc.argtypes = L.lbm_solve2d.argtypes
         L.lbm_solve2d_noalloc.restype = C.c_int
         L.lbm_batch_create.argtypes = [vp, C.POINTER(vp), C.c_int, C.c_longlong, C.c_int]

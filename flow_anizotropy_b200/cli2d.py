@@ -56,10 +56,11 @@ def mu_2d(tau: float) -> float:
     return float(np.float32(0.33 * (float(np.float32(tau)) - 0.5)))
 
 
-def run(argv) -> int:
+def parse(argv):
+    """(structure, resultfile, cfg) from the lbm2d-perm argv; None after --help."""
     if len(argv) < 2:
         sys.stderr.write(USAGE)
-        return 1
+        raise Die("missing arguments")
     structure, resultfile = argv[0], argv[1]
     cfg = dict(ff=1.0, eps=1e-3, lag=5000, hold=3, min_steps=10000, max_steps=500000,
                avg_steps=20000, avg_sample=50, qfloor=1e-2, ksigma=3.0, velocity="",
@@ -98,7 +99,7 @@ def run(argv) -> int:
             cfg["size"] = (strtol(v[0]), strtol(v[1]))
         elif a in ("-h", "--help"):
             sys.stderr.write(USAGE)
-            return 0
+            return None
         else:
             sys.stderr.write(USAGE)
             raise Die("unknown option " + a)
@@ -106,6 +107,17 @@ def run(argv) -> int:
     if cfg["lag"] <= 0 or cfg["avg_sample"] <= 0:
         raise Die("--lag and --avg-sample must be positive")
 
+    return structure, resultfile, cfg
+
+
+def run(argv) -> int:
+    if len(argv) < 2:
+        sys.stderr.write(USAGE)
+        return 1
+    parsed = parse(argv)
+    if parsed is None:
+        return 0
+    structure, resultfile, cfg = parsed
     F = S.FX_BASE * cfg["ff"]
     nx, ny = cfg["size"]
     try:

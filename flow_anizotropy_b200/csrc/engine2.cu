@@ -235,6 +235,106 @@ extern "C" int lbm_solve2d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny,
     return out;
 }
 
+// Several structures of one cell size, each with the same forcing directions,
+// advanced by one launch per step: the work list covers every (structure,
+// direction) solve, each with its own mask, controller and flux partials, so
+// every result equals the structure solved alone.
+extern "C" int lbm_solve2d_many(lbm_ctx *ctx, int nstruct, const uint8_t *solids, int nx, int ny, int ndir,
+                                const double *forces, const lbm_params2d *params, lbm_result2d *results)
+{
+    if (!ctx) return LBM_EINPUT;
+    if (!solids || !forces || !params || !results || ndir <= 0 || nstruct <= 0)
+        return lbm_fail_input(ctx, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    if (nx <= 0 || ny <= 0) return lbm_fail_input(ctx, "bad dimensions");
+    const long long nn = (long long)nx * ny;
+    if (nn >= (1ll << 27)) return lbm_fail_input(ctx, "2D lattice too large");
+    const lbm_params2d p = *params;
+    int rc = check_params2d(ctx, p);
+    if (rc) return rc;
+    const int nsolve = nstruct * ndir;
+    std::vector<DevMem> masks;
+    masks.reserve(nstruct);
+    std::vector<Solve2> hs(nsolve);
+    std::vector<State2> hst(nsolve);
+    std::vector<DevMem> bufs;
+    bufs.reserve(4 * (size_t)nsolve);
+    DevMem d_states(ctx->stream), d_solves(ctx->stream), d_work(ctx->stream), fr(ctx->stream);
+    CK(d_states.alloc(sizeof(State2) * nsolve));
+    for (int k = 0; k < nstruct; ++k) {
+        masks.emplace_back(ctx->stream);
+        long long npore = 0;
+        rc = lbm_upload_mask(ctx, solids + nn * k, nx, ny, masks.back(), npore);
+        if (rc) {
+            ctx->err = "structure " + std::to_string(k) + ": " + ctx->err;
+            return rc;
+        }
+        for (int j = 0; j < ndir; ++j) {
+            const int id = k * ndir + j;
+            Solve2 &S = hs[id];
+            fill_solve2(S, nx, ny, forces + 2 * j, p);
+            for (int b = 0; b < 4; ++b) bufs.emplace_back(ctx->stream);
+            DevMem *B = &bufs[4 * (size_t)id];
+            CK(B[0].alloc(sizeof(float) * Q2 * (size_t)S.plane));
+            CK(B[1].alloc(sizeof(double) * 2 * (size_t)S.ntiles));
+            CK(B[2].alloc(sizeof(float) * 2 * (size_t)nn));
+            CK(B[3].alloc(sizeof(float) * 2 * (size_t)nn));
+            CK(cudaMemsetAsync(B[2].p, 0, sizeof(float) * 2 * (size_t)nn, ctx->stream));
+            CK(cudaMemsetAsync(B[3].p, 0, sizeof(float) * 2 * (size_t)nn, ctx->stream));
+            S.A = static_cast<float *>(B[0].p);
+            S.partials = static_cast<double *>(B[1].p);
+            S.snap = static_cast<float *>(B[2].p);
+            S.last = static_cast<float *>(B[3].p);
+            S.mask = static_cast<const uint32_t *>(masks.back().p);
+            S.st = static_cast<State2 *>(d_states.p) + id;
+            init_state2(hst[id], S.c);
+            init2d_kernel<<<256, 256, 0, ctx->stream>>>(S.A, S.plane, S.nn);
+            CK(cudaGetLastError());
+        }
+    }
+    std::vector<int2> work;
+    for (int id = 0; id < nsolve; ++id)
+        for (int t = 0; t < hs[id].ntiles; ++t) work.push_back(make_int2(id, t));
+    CK(d_solves.alloc(sizeof(Solve2) * nsolve));
+    CK(d_work.alloc(sizeof(int2) * work.size()));
+    CK(cudaMemcpyAsync(d_solves.p, hs.data(), sizeof(Solve2) * nsolve, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_work.p, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_states.p, hst.data(), sizeof(State2) * nsolve, cudaMemcpyHostToDevice, ctx->stream));
+    rc = run_plain2d(ctx, hs, static_cast<Solve2 *>(d_solves.p), static_cast<State2 *>(d_states.p),
+                     static_cast<const int2 *>(d_work.p), (int)work.size(), hst);
+    if (rc) return rc;
+    CK(fr.alloc(sizeof(double) * 2 * nsolve));
+    CK(cudaMemsetAsync(fr.p, 0, sizeof(double) * 2 * nsolve, ctx->stream));
+    for (int id = 0; id < nsolve; ++id) {
+        fieldres2d_kernel<<<64, TPB, 0, ctx->stream>>>(hs[id].snap, hs[id].last, hs[id].nn,
+                                                       static_cast<double *>(fr.p) + 2 * id);
+        CK(cudaGetLastError());
+    }
+    std::vector<double> frh(2 * (size_t)nsolve);
+    CK(cudaMemcpyAsync(frh.data(), fr.p, sizeof(double) * 2 * nsolve, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    int out = LBM_OK;
+    for (int id = 0; id < nsolve; ++id) {
+        const State2 &st = hst[id];
+        lbm_result2d &r = results[id];
+        r.q[0] = st.q[0]; r.q[1] = st.q[1];
+        r.se[0] = st.se[0]; r.se[1] = st.se[1];
+        r.steps = st.steps;
+        r.converged = st.converged;
+        r.status = st.status;
+        const double num = frh[2 * id], den = frh[2 * id + 1];
+        r.fieldres = den > 0.0 ? (double)(float)std::sqrt(num / den) : 10.0;
+        if (st.status) {
+            ctx->err = "non-finite flux in structure " + std::to_string(id / ndir) + " run " +
+                       std::to_string(id % ndir) + " at step " + std::to_string(st.steps);
+            out = LBM_EINPUT;
+        } else if (!st.converged && out == LBM_OK) {
+            out = LBM_NOT_CONVERGED;
+        }
+    }
+    return out;
+}
+
 extern "C" int lbm_debug_steps2d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny,
                                  const double force[2], double tau, long long nsteps,
                                  float *f_out, float *u_out, double q_out[2])

@@ -158,6 +158,27 @@ def solve2d(solid, forces, params: Params2D | None = None, velocity: bool = Fals
     return out, rc, vel
 
 
+def solve2d_many(solids, forces, params: Params2D | None = None, device: int = 0):
+    """Several structures of one cell size (array [n, y, x]) along the same
+    forcing directions in one launch per step; returns (runs [n][ndir], rc).
+    Each structure's results equal solve2d of it alone."""
+    params = params or Params2D()
+    ctx = _lib.context(device)
+    arr = np.ascontiguousarray(solids, dtype=np.uint8)
+    n, ny, nx = arr.shape
+    F = np.ascontiguousarray(np.asarray(forces, dtype=np.float64).reshape(-1, 2))
+    ndir = F.shape[0]
+    res = (_lib.Result2D * (n * ndir))()
+    P = params.to_c()
+    rc = ctx.L.lbm_solve2d_many(ctx.h, n, arr.ctypes.data_as(C.POINTER(C.c_uint8)), nx, ny, ndir,
+                                F.ctypes.data_as(C.POINTER(C.c_double)), C.byref(P), res)
+    ctx.check(rc, ok=(_lib.LBM_OK, _lib.LBM_NOT_CONVERGED))
+    runs = [[Result2D(q=np.array(r.q[:]), se=np.array(r.se[:]), steps=int(r.steps), converged=int(r.converged),
+                      status=int(r.status), fieldres=float(r.fieldres)) for r in res[k * ndir:(k + 1) * ndir]]
+            for k in range(n)]
+    return runs, rc
+
+
 def debug_steps3d(solid, force, nsteps, tau=1.0, precision="fp64", variant=0, device=0):
     """Exactly ``nsteps`` steps; returns (f [z,y,x,19] float64, u [z,y,x,3] float32, q)."""
     ctx = _lib.context(device)

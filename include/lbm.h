@@ -145,6 +145,14 @@ int lbm_solve2d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny,
                 int ndir, const double *forces, const lbm_params2d *params,
                 lbm_result2d *results, float *vel_out);
 
+/* nstruct structures of one nx x ny cell (solids: nstruct x ny x nx), each
+ * solved along the same ndir forcing directions, all advanced by one launch
+ * per step; results: nstruct x ndir, structure-major, each equal to
+ * lbm_solve2d of that structure alone.  Replaces nstruct lbm2d-perm processes
+ * of scripts/solve_permeability.py:29-46 (LMB2d/main.cpp:99-235 each). */
+int lbm_solve2d_many(lbm_ctx *ctx, int nstruct, const uint8_t *solids, int nx, int ny, int ndir,
+                     const double *forces, const lbm_params2d *params, lbm_result2d *results);
+
 /* Largest input of lbm_solve2d_noalloc: the reference's fixed 256 x 256 cell
  * (LMB2d/lbm.h:24-26) and its two forcing directions (LMB2d/main.cpp:323-324). */
 #define LBM_NOALLOC2D_MAX_CELLS 65536
