@@ -190,6 +190,7 @@ struct StoreF64 {
     __device__ static __forceinline__ const W *word(const T *p) { return p; }
     __device__ static __forceinline__ C unword(W w, unsigned) { return w; }
     static constexpr bool shifted = false;
+    static constexpr bool stochastic = false;
     static constexpr int code = 0;
     __device__ static __forceinline__ C ld(const T *p) { return __ldcs(p); }
     __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, v); }
@@ -200,6 +201,7 @@ struct StoreF32 {
     __device__ static __forceinline__ const W *word(const T *p) { return p; }
     __device__ static __forceinline__ C unword(W w, unsigned) { return w; }
     static constexpr bool shifted = true;
+    static constexpr bool stochastic = false;
     static constexpr int code = 1;
     __device__ static __forceinline__ C ld(const T *p) { return __ldcs(p); }
     __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, v); }
@@ -219,6 +221,16 @@ struct StoreF16 {
     static constexpr int code = 2;
     __device__ static __forceinline__ C ld(const T *p) { return __half2float(__ldcs(p)); }
     __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, __float2half_rn(v)); }
+    // stochastic rounding: 13 random bits added below the half mantissa of the
+    // float, then truncated, round the magnitude up with probability equal to
+    // its distance from the lower half (unbiased, so increments smaller than
+    // half an ulp accumulate instead of being rounded away every step)
+    static constexpr bool stochastic = true;
+    __device__ static __forceinline__ void st_sr(T *p, C v, uint32_t rnd)
+    {
+        const uint32_t b = (__float_as_uint(v) + (rnd & 0x1fffu)) & ~0x1fffu;
+        __stcs(p, __float2half_rz(__uint_as_float(b)));
+    }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 struct StoreBF16 {
@@ -235,6 +247,13 @@ struct StoreBF16 {
     static constexpr int code = 3;
     __device__ static __forceinline__ C ld(const T *p) { return __bfloat162float(__ldcs(p)); }
     __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, __float2bfloat16_rn(v)); }
+    // stochastic rounding (as StoreF16, with the 16 bits below the bfloat16 mantissa)
+    static constexpr bool stochastic = true;
+    __device__ static __forceinline__ void st_sr(T *p, C v, uint32_t rnd)
+    {
+        const uint32_t b = (__float_as_uint(v) + (rnd & 0xffffu)) & ~0xffffu;
+        __stcs(p, __float2bfloat16_rz(__uint_as_float(b)));
+    }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 

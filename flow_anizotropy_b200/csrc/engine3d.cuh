@@ -447,6 +447,28 @@ __host__ __device__ constexpr Variant even_f64(int v)
 // list (and its partials), so both use TPB * TILE_NPT voxels per tile
 constexpr int TILE_NPT = 2;
 
+// Store of a post-collision population at lattice slot `slot` of step n: the
+// 16-bit storage types round stochastically, with random bits from a hash of
+// (slot, n) (deterministic: a solve gives the same bits alone or in a batch),
+// the others round to nearest.
+__device__ __forceinline__ uint32_t sr_bits(unsigned slot, long long n)
+{
+    uint32_t h = slot * 0x9e3779b1u ^ (uint32_t)n * 0x85ebca77u ^ (uint32_t)(n >> 32) * 0xc2b2ae3du;
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    return h;
+}
+
+template <class ST>
+__device__ __forceinline__ void store_pop(typename ST::T *A, unsigned slot, typename ST::C v, long long n)
+{
+    if constexpr (ST::stochastic) ST::st_sr(A + slot, v, sr_bits(slot, n));
+    else ST::st(A + slot, v);
+}
+
 // Collision dispatch: FP64 keeps the reference's arithmetic; reduced-precision
 // storage uses the pair-symmetric FP32 operator, specialised for tau = 1.
 template <class ST, bool W1, class Cp>
@@ -495,7 +517,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
                 Cp ux, uy, uz;
                 collide3<ST, W1>(g[j], S, ux, uy, uz);
 #pragma unroll
-                for (int k = 0; k < Q3; ++k) ST::st(A + (opp3(k) * P + iv[j]), g[j][k]);
+                for (int k = 0; k < Q3; ++k) store_pop<ST>(A, opp3(k) * P + iv[j], g[j][k], n);
                 acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
             }
         }
@@ -559,11 +581,11 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
             }
             Cp ux, uy, uz;
             collide3<ST, W1>(g, S, ux, uy, uz);
-            ST::st(A + i, g[0]);
+            store_pop<ST>(A, i, g[0], n);
 #pragma unroll
             for (int k = 1; k < Q3; ++k) {
                 const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                ST::st(A + dst, g[k]);
+                store_pop<ST>(A, dst, g[k], n);
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
@@ -641,11 +663,12 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_group_kernel(const Step
                 T *__restrict__ A = static_cast<T *>(S.A);
                 Cp ux, uy, uz;
                 collide3<ST, W1>(g[d], S, ux, uy, uz);
-                ST::st(A + i, g[d][0]);
+                const long long nd = S.st->s_base + a.step + 1;
+                store_pop<ST>(A, i, g[d][0], nd);
 #pragma unroll
                 for (int k = 1; k < Q3; ++k) {
                     const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                    ST::st(A + dst, g[d][k]);
+                    store_pop<ST>(A, dst, g[d][k], nd);
                 }
                 if ((redm >> d) & 1u) {
                     sacc[d][0][threadIdx.x] += (double)ux;
@@ -728,11 +751,11 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const Step
             collide3<ST, W1>(g, S, ux, uy, uz);
             CNb nb;
             meta_nbrs(S, i, mr[j], mr2[j], nb);
-            ST::st(A + i, g[0]);
+            store_pop<ST>(A, i, g[0], n);
 #pragma unroll
             for (int k = 1; k < Q3; ++k) {
                 const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                ST::st(A + dst, g[k]);
+                store_pop<ST>(A, dst, g[k], n);
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
