@@ -221,15 +221,17 @@ struct StoreF16 {
     static constexpr int code = 2;
     __device__ static __forceinline__ C ld(const T *p) { return __half2float(__ldcs(p)); }
     __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, __float2half_rn(v)); }
-    // stochastic rounding: 13 random bits added below the half mantissa of the
-    // float, then truncated, round the magnitude up with probability equal to
-    // its distance from the lower half (unbiased, so increments smaller than
-    // half an ulp accumulate instead of being rounded away every step)
+    // stochastic rounding (sm_100a cvt.rs with random bits; the product bits
+    // in `rnd` are rotated so that its well-mixed high half is used): rounds up
+    // with probability equal to the distance from the lower half, unbiased, so
+    // increments smaller than half an ulp accumulate instead of being rounded
+    // away every step
     static constexpr bool stochastic = true;
     __device__ static __forceinline__ void st_sr(T *p, C v, uint32_t rnd)
     {
-        const uint32_t b = (__float_as_uint(v) + (rnd & 0x1fffu)) & ~0x1fffu;
-        __stcs(p, __float2half_rz(__uint_as_float(b)));
+        uint32_t d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(0.0f), "f"(v), "r"(__funnelshift_l(rnd, rnd, 16)));
+        __stcs(p, __ushort_as_half((unsigned short)(d & 0xffffu)));
     }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
@@ -247,12 +249,13 @@ struct StoreBF16 {
     static constexpr int code = 3;
     __device__ static __forceinline__ C ld(const T *p) { return __bfloat162float(__ldcs(p)); }
     __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, __float2bfloat16_rn(v)); }
-    // stochastic rounding (as StoreF16, with the 16 bits below the bfloat16 mantissa)
+    // stochastic rounding (as StoreF16)
     static constexpr bool stochastic = true;
     __device__ static __forceinline__ void st_sr(T *p, C v, uint32_t rnd)
     {
-        const uint32_t b = (__float_as_uint(v) + (rnd & 0xffffu)) & ~0xffffu;
-        __stcs(p, __float2bfloat16_rz(__uint_as_float(b)));
+        uint32_t d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(0.0f), "f"(v), "r"(__funnelshift_l(rnd, rnd, 16)));
+        __stcs(p, __ushort_as_bfloat16((unsigned short)(d & 0xffffu)));
     }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };

@@ -447,13 +447,14 @@ __host__ __device__ constexpr Variant even_f64(int v)
 // list (and its partials), so both use TPB * TILE_NPT voxels per tile
 constexpr int TILE_NPT = 2;
 
-// Store of a post-collision population at lattice slot `slot` of step n: the
-// 16-bit storage types round stochastically, with random bits from a hash of
-// (slot, n) (deterministic: a solve gives the same bits alone or in a batch),
-// the others round to nearest.
-__device__ __forceinline__ uint32_t sr_bits(unsigned slot, long long n)
+// Store of population k of pore voxel i at lattice slot `slot` in step n: the
+// 16-bit storage types round stochastically, the others to nearest.  The
+// random bits are a per-(voxel, step) hash times an odd per-direction
+// constant (its high bits are used), so each store draws fresh bits for one
+// multiply, and a solve gives the same bits alone or in a batch.
+__device__ __forceinline__ uint32_t sr_voxel(unsigned i, long long n)
 {
-    uint32_t h = slot * 0x9e3779b1u ^ (uint32_t)n * 0x85ebca77u ^ (uint32_t)(n >> 32) * 0xc2b2ae3du;
+    uint32_t h = i * 0x9e3779b1u ^ (uint32_t)n * 0x85ebca77u ^ (uint32_t)(n >> 32) * 0xc2b2ae3du;
     h ^= h >> 16;
     h *= 0x7feb352du;
     h ^= h >> 15;
@@ -463,10 +464,17 @@ __device__ __forceinline__ uint32_t sr_bits(unsigned slot, long long n)
 }
 
 template <class ST>
-__device__ __forceinline__ void store_pop(typename ST::T *A, unsigned slot, typename ST::C v, long long n)
+__device__ __forceinline__ void store_pop(typename ST::T *A, unsigned slot, typename ST::C v, uint32_t hv, int k)
 {
-    if constexpr (ST::stochastic) ST::st_sr(A + slot, v, sr_bits(slot, n));
+    if constexpr (ST::stochastic) ST::st_sr(A + slot, v, hv * (0x9e3779b1u * (2u * (uint32_t)k + 1u)));
     else ST::st(A + slot, v);
+}
+
+template <class ST>
+__device__ __forceinline__ uint32_t voxel_bits(unsigned i, long long n)
+{
+    if constexpr (ST::stochastic) return sr_voxel(i, n);
+    else return 0u;
 }
 
 // Collision dispatch: FP64 keeps the reference's arithmetic; reduced-precision
@@ -516,8 +524,11 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
                 if (!vv[j]) continue;
                 Cp ux, uy, uz;
                 collide3<ST, W1>(g[j], S, ux, uy, uz);
+                {
+                    const uint32_t hv = voxel_bits<ST>(iv[j], n);
 #pragma unroll
-                for (int k = 0; k < Q3; ++k) store_pop<ST>(A, opp3(k) * P + iv[j], g[j][k], n);
+                    for (int k = 0; k < Q3; ++k) store_pop<ST>(A, opp3(k) * P + iv[j], g[j][k], hv, k);
+                }
                 acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
             }
         }
@@ -581,11 +592,12 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
             }
             Cp ux, uy, uz;
             collide3<ST, W1>(g, S, ux, uy, uz);
-            store_pop<ST>(A, i, g[0], n);
+            const uint32_t hv = voxel_bits<ST>(i, n);
+            store_pop<ST>(A, i, g[0], hv, 0);
 #pragma unroll
             for (int k = 1; k < Q3; ++k) {
                 const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                store_pop<ST>(A, dst, g[k], n);
+                store_pop<ST>(A, dst, g[k], hv, k);
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
@@ -663,12 +675,12 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_group_kernel(const Step
                 T *__restrict__ A = static_cast<T *>(S.A);
                 Cp ux, uy, uz;
                 collide3<ST, W1>(g[d], S, ux, uy, uz);
-                const long long nd = S.st->s_base + a.step + 1;
-                store_pop<ST>(A, i, g[d][0], nd);
+                const uint32_t hv = voxel_bits<ST>(i, S.st->s_base + a.step + 1);
+                store_pop<ST>(A, i, g[d][0], hv, 0);
 #pragma unroll
                 for (int k = 1; k < Q3; ++k) {
                     const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                    store_pop<ST>(A, dst, g[d][k], nd);
+                    store_pop<ST>(A, dst, g[d][k], hv, k);
                 }
                 if ((redm >> d) & 1u) {
                     sacc[d][0][threadIdx.x] += (double)ux;
@@ -751,11 +763,12 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const Step
             collide3<ST, W1>(g, S, ux, uy, uz);
             CNb nb;
             meta_nbrs(S, i, mr[j], mr2[j], nb);
-            store_pop<ST>(A, i, g[0], n);
+            const uint32_t hv = voxel_bits<ST>(i, n);
+            store_pop<ST>(A, i, g[0], hv, 0);
 #pragma unroll
             for (int k = 1; k < Q3; ++k) {
                 const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                store_pop<ST>(A, dst, g[k], n);
+                store_pop<ST>(A, dst, g[k], hv, k);
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
