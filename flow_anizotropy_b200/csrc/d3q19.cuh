@@ -206,6 +206,16 @@ struct StoreF32 {
     __device__ static __forceinline__ C ld(const T *p) { return __ldcs(p); }
     __device__ static __forceinline__ void st(T *p, C v) { __stcs(p, v); }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
+    // two adjacent slots (p 8-byte aligned) in one access
+    __device__ static __forceinline__ void ld2(const T *p, C &lo, C &hi)
+    {
+        const float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
+        lo = v.x; hi = v.y;
+    }
+    __device__ static __forceinline__ void st2(T *p, C lo, C hi, uint32_t, uint32_t)
+    {
+        __stcs(reinterpret_cast<float2 *>(p), make_float2(lo, hi));
+    }
 };
 struct StoreF16 {
     using T = __half; using C = float; using W = uint32_t;
@@ -233,6 +243,22 @@ struct StoreF16 {
         asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(0.0f), "f"(v), "r"(__funnelshift_l(rnd, rnd, 16)));
         __stcs(p, __ushort_as_half((unsigned short)(d & 0xffffu)));
     }
+    // two adjacent slots (p 4-byte aligned) in one access; the pair store
+    // rounds each half with the random bits st_sr would give it (the low 16
+    // of its rotated bits), so results equal two single stores
+    __device__ static __forceinline__ void ld2(const T *p, C &lo, C &hi)
+    {
+        const uint32_t w = __ldcs(reinterpret_cast<const unsigned int *>(p));
+        lo = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+        hi = __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+    }
+    __device__ static __forceinline__ void st2(T *p, C lo, C hi, uint32_t rlo, uint32_t rhi)
+    {
+        const uint32_t rb = (__funnelshift_l(rhi, rhi, 16) << 16) | (__funnelshift_l(rlo, rlo, 16) & 0xffffu);
+        uint32_t d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rb));
+        __stcs(reinterpret_cast<unsigned int *>(p), d);
+    }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };
 struct StoreBF16 {
@@ -256,6 +282,19 @@ struct StoreBF16 {
         uint32_t d;
         asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(0.0f), "f"(v), "r"(__funnelshift_l(rnd, rnd, 16)));
         __stcs(p, __ushort_as_bfloat16((unsigned short)(d & 0xffffu)));
+    }
+    __device__ static __forceinline__ void ld2(const T *p, C &lo, C &hi)
+    {
+        const uint32_t w = __ldcs(reinterpret_cast<const unsigned int *>(p));
+        lo = __bfloat162float(__ushort_as_bfloat16((unsigned short)(w & 0xffffu)));
+        hi = __bfloat162float(__ushort_as_bfloat16((unsigned short)(w >> 16)));
+    }
+    __device__ static __forceinline__ void st2(T *p, C lo, C hi, uint32_t rlo, uint32_t rhi)
+    {
+        const uint32_t rb = (__funnelshift_l(rhi, rhi, 16) << 16) | (__funnelshift_l(rlo, rlo, 16) & 0xffffu);
+        uint32_t d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rb));
+        __stcs(reinterpret_cast<unsigned int *>(p), d);
     }
     __host__ __device__ static constexpr double init(int) { return 0.0; }
 };

@@ -420,11 +420,16 @@ __device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, const uin
 // (NVAR_EVEN_LP for the reduced-precision storage, which adds the grouped
 // even kernels); lbm_tune3d times them on the actual structure.
 struct Variant { int npt, minb; };
-constexpr int NVAR_ODD = 3, NVAR_EVEN = 6, NVAR_EVEN_LP = 8;
-constexpr int NVAR_LP = NVAR_ODD * NVAR_EVEN_LP, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
+constexpr int NVAR_ODD = 3, NVAR_ODD_LP = 4, NVAR_EVEN = 6, NVAR_EVEN_LP = 8;
+constexpr int NVAR_LP = NVAR_ODD_LP * NVAR_EVEN_LP, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
 constexpr int MAX_GROUP = 3;    // directions per grouped even step
 inline int nvar_even(int prec) { return prec == 0 ? NVAR_EVEN : NVAR_EVEN_LP; }
-__host__ __device__ constexpr Variant odd_lp(int v) { return v == 0 ? Variant{1, 4} : v == 1 ? Variant{1, 5} : Variant{2, 2}; }
+// odd variants: 0-1 one voxel per thread, 2 two voxels a tile-half apart, 3
+// two adjacent voxels per thread with paired (vector) slot accesses
+__host__ __device__ constexpr Variant odd_lp(int v)
+{
+    return v == 0 ? Variant{1, 4} : v == 1 ? Variant{1, 5} : Variant{2, 2};
+}
 // even variants: 0-1 read the neighbour record (META), 2-3 compute ranks from
 // the mask, 4-5 read the record and stage their gathers with cp.async, 6-7
 // are grouped (one rank computation for all directions of a structure; 6
@@ -463,10 +468,13 @@ __device__ __forceinline__ uint32_t sr_voxel(unsigned i, long long n)
     return h;
 }
 
+// random bits of store k of a voxel with per-(voxel, step) hash hv
+__device__ __forceinline__ uint32_t dir_bits(uint32_t hv, int k) { return hv * (0x9e3779b1u * (2u * (uint32_t)k + 1u)); }
+
 template <class ST>
 __device__ __forceinline__ void store_pop(typename ST::T *A, unsigned slot, typename ST::C v, uint32_t hv, int k)
 {
-    if constexpr (ST::stochastic) ST::st_sr(A + slot, v, hv * (0x9e3779b1u * (2u * (uint32_t)k + 1u)));
+    if constexpr (ST::stochastic) ST::st_sr(A + slot, v, dir_bits(hv, k));
     else ST::st(A + slot, v);
 }
 
@@ -531,6 +539,51 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
                 }
                 acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
             }
+        }
+        if (red) finish_tile(S, item.y, n, acc, sh);
+    }
+}
+
+// Odd (local) step with two adjacent pore voxels (i, i + 1), i even, per
+// thread: every slot pair of a plane is one aligned 8-byte (FP32) or 4-byte
+// (16-bit) access, and the 16-bit types round both values with one cvt.rs
+// fed with the bits each would get alone, so the populations equal those of
+// step3d_odd_kernel (the flux partials are summed in another order).  The
+// partner of the last voxel of an odd-sized lattice is a padding slot (the
+// plane stride is a multiple of 64); it is read and written but never used.
+template <class ST, int MINB, bool W1>
+__global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    using Cp = typename ST::C;
+    static_assert(TILE_NPT == 2, "a tile is one voxel pair per thread");
+    __shared__ double sh[TPB / 32][3];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S = a.solves[item.x];
+        const int phase = S.st->phase;
+        if (phase >= PH_DONE) continue;
+        const long long n = S.st->s_base + a.step + 1;
+        const bool red = needs_reduction(S.c, phase, n);
+        T *__restrict__ A = static_cast<T *>(S.A);
+        const unsigned P = (unsigned)S.plane;
+        double acc[3] = {0.0, 0.0, 0.0};
+        const unsigned i0 = (unsigned)(item.y * (TPB * TILE_NPT) + 2 * threadIdx.x);
+        if (i0 < (unsigned)S.nfluid) {
+            const bool v1 = i0 + 1u < (unsigned)S.nfluid;
+            Cp g0[Q3], g1[Q3];
+#pragma unroll
+            for (int k = 0; k < Q3; ++k) ST::ld2(A + (k * P + i0), g0[k], g1[k]);
+            Cp ux0, uy0, uz0, ux1 = Cp(0), uy1 = Cp(0), uz1 = Cp(0);
+            collide3<ST, W1>(g0, S, ux0, uy0, uz0);
+            if (v1) collide3<ST, W1>(g1, S, ux1, uy1, uz1);
+            const uint32_t h0 = voxel_bits<ST>(i0, n), h1 = voxel_bits<ST>(i0 + 1u, n);
+#pragma unroll
+            for (int k = 0; k < Q3; ++k)
+                ST::st2(A + (opp3(k) * P + i0), g0[k], g1[k], dir_bits(h0, k), dir_bits(h1, k));
+            acc[0] += (double)ux0; acc[1] += (double)uy0; acc[2] += (double)uz0;
+            if (v1) { acc[0] += (double)ux1; acc[1] += (double)uy1; acc[2] += (double)uz1; }
         }
         if (red) finish_tile(S, item.y, n, acc, sh);
     }

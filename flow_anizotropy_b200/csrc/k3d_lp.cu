@@ -9,6 +9,7 @@ cudaError_t launch_canon3d_f64(const Solve3 &S, long long done, double *f, float
 int max_blocks_f64(int variant, bool odd);
 
 #define LBM_ODD(ST, V, W) step3d_odd_kernel<ST, odd_lp(V).npt, odd_lp(V).minb, W>
+#define LBM_ODDP(ST, W) step3d_odd_pair_kernel<ST, odd_lp(3).minb, W>
 #define LBM_EVEN(ST, V, W) step3d_even_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 #define LBM_EVENA(ST, V, W) step3d_even_async_kernel<ST, even_lp(V).minb, W>
 #define LBM_EVENG(ST, V, W) step3d_even_group_kernel<ST, even_lp(V).minb, W, even_meta(V)>
@@ -22,7 +23,8 @@ static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const S
         switch (vo) {
         case 0: LBM_ODD(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
         case 1: LBM_ODD(ST, 1, W)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_ODD(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 2: LBM_ODD(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_ODDP(ST, W)<<<grid, TPB, 0, s>>>(a); break;
         }
     } else {
         switch (ve) {
@@ -54,7 +56,7 @@ static int occ(int v, bool odd)
 {
     const int vo = v / NVAR_EVEN_LP, ve = v % NVAR_EVEN_LP;
     const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(ST, 0, true) : vo == 1 ? (const void *)LBM_ODD(ST, 1, true)
-                                                                        : (const void *)LBM_ODD(ST, 2, true))
+                           : vo == 2 ? (const void *)LBM_ODD(ST, 2, true) : (const void *)LBM_ODDP(ST, true))
                         : (ve == 0 ? (const void *)LBM_EVEN(ST, 0, true) : ve == 1 ? (const void *)LBM_EVEN(ST, 1, true)
                            : ve == 2 ? (const void *)LBM_EVEN(ST, 2, true) : ve == 3 ? (const void *)LBM_EVEN(ST, 3, true)
                            : ve == 4 ? (const void *)LBM_EVENA(ST, 4, true) : ve == 5 ? (const void *)LBM_EVENA(ST, 5, true)
