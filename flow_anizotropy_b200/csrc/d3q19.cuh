@@ -110,70 +110,131 @@ __device__ __forceinline__ void collide_ref64(double (&g)[Q3], const Phys3 &P,
 // ~1e-2 in k; working in scaled units leaves FP16 loads and stores a bare
 // conversion.  W1: tau == 1, where h drops out of the update.
 // ---------------------------------------------------------------------------
-template <bool W1>
-__device__ __forceinline__ void collide_pairs(float (&h)[Q3], const Phys3 &P, float s, float is,
-                                              float &ux, float &uy, float &uz)
+//
+// Every operation is written out with its rounding (no contraction left to
+// the compiler), and the operator is a template over the arithmetic: F32x1
+// evaluates one voxel, F32x2 two voxels at once with the sm_100 packed FP32
+// instructions (one issue slot per pair of lanes).  Both round each value
+// identically, so a kernel that collides voxel pairs gives the same bits as
+// one that collides them one at a time.
+struct F32x1 {
+    using V = float;
+    __device__ static __forceinline__ V add(V a, V b) { return __fadd_rn(a, b); }
+    __device__ static __forceinline__ V sub(V a, V b) { return __fsub_rn(a, b); }
+    __device__ static __forceinline__ V mul(V a, V b) { return __fmul_rn(a, b); }
+    __device__ static __forceinline__ V fma(V a, V b, V c) { return __fmaf_rn(a, b, c); }
+    __device__ static __forceinline__ V neg(V a) { return -a; }
+    __device__ static __forceinline__ V splat(float x) { return x; }
+    __device__ static __forceinline__ V recip(V a) { return __frcp_rn(a); }
+};
+struct F32x2 {
+    using V = float2;
+    __device__ static __forceinline__ V add(V a, V b) { return __fadd2_rn(a, b); }
+    // a - b as b * (-1) + a: the product is exact, so one rounding, as __fsub_rn
+    __device__ static __forceinline__ V sub(V a, V b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+    __device__ static __forceinline__ V mul(V a, V b) { return __fmul2_rn(a, b); }
+    __device__ static __forceinline__ V fma(V a, V b, V c) { return __ffma2_rn(a, b, c); }
+    __device__ static __forceinline__ V neg(V a) { return make_float2(-a.x, -a.y); }
+    __device__ static __forceinline__ V splat(float x) { return make_float2(x, x); }
+    __device__ static __forceinline__ V recip(V a) { return make_float2(__frcp_rn(a.x), __frcp_rn(a.y)); }
+};
+
+// sign * v accumulated into acc; `first` starts the sum with the term itself
+template <class O>
+__device__ __forceinline__ void signed_acc(typename O::V &acc, bool &first, int sign, typename O::V v)
 {
+    if (!sign) return;
+    if (first) acc = sign > 0 ? v : O::neg(v);
+    else acc = sign > 0 ? O::add(acc, v) : O::sub(acc, v);
+    first = false;
+}
+
+__device__ __forceinline__ float signed_sum3(int cx, int cy, int cz, float x, float y, float z)
+{
+    float r = 0.0f;
+    bool first = true;
+    signed_acc<F32x1>(r, first, cx, x);
+    signed_acc<F32x1>(r, first, cy, y);
+    signed_acc<F32x1>(r, first, cz, z);
+    return r;
+}
+
+template <bool W1, class O>
+__device__ __forceinline__ void collide_pairs(typename O::V (&h)[Q3], const Phys3 &P, float s, float is,
+                                              typename O::V &ux, typename O::V &uy, typename O::V &uz)
+{
+    using V = typename O::V;
     // pair sums and differences; the odd member k of each pair is the "+" one
-    float sm[9], df[9];
+    V sm[9], df[9];
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
-        sm[p] = h[2 * p + 1] + h[2 * p + 2];
-        df[p] = h[2 * p + 1] - h[2 * p + 2];
+        sm[p] = O::add(h[2 * p + 1], h[2 * p + 2]);
+        df[p] = O::sub(h[2 * p + 1], h[2 * p + 2]);
     }
-    float drs = h[0];
+    V drs = h[0];
 #pragma unroll
-    for (int p = 0; p < 9; ++p) drs += sm[p];
-    float jx = 0.f, jy = 0.f, jz = 0.f;
+    for (int p = 0; p < 9; ++p) drs = O::add(drs, sm[p]);
+    V jx = O::splat(0.0f), jy = O::splat(0.0f), jz = O::splat(0.0f);
+    bool fx = true, fy = true, fz = true;
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
         const int k = 2 * p + 1;
-        if (ex3(k)) jx += ex3(k) > 0 ? df[p] : -df[p];
-        if (ey3(k)) jy += ey3(k) > 0 ? df[p] : -df[p];
-        if (ez3(k)) jz += ez3(k) > 0 ? df[p] : -df[p];
+        signed_acc<O>(jx, fx, ex3(k), df[p]);
+        signed_acc<O>(jy, fy, ey3(k), df[p]);
+        signed_acc<O>(jz, fz, ez3(k), df[p]);
     }
+    // per-solve scalars (the same for every voxel)
     const float Fx = P.Ff[0], Fy = P.Ff[1], Fz = P.Ff[2];
-    const float dr = drs * is;
-    const float rho = 1.0f + dr;
-    const float ir = 1.0f / rho;
-    ux = fmaf(jx, is, 0.5f * Fx) * ir;
-    uy = fmaf(jy, is, 0.5f * Fy) * ir;
-    uz = fmaf(jz, is, 0.5f * Fz) * ir;
-    const float u2 = ux * ux + uy * uy + uz * uz;
-    const float uF = ux * Fx + uy * Fy + uz * Fz;
-    const float pr = P.preff;
-    const float srho = s * rho;
-    // per-node constants in scaled units
-    const float c1 = drs - 1.5f * srho * u2 - 3.0f * s * pr * uF;   // symmetric, eu = eF = 0 part
-    const float r45 = 4.5f * srho, r3 = 3.0f * srho;
-    const float p9 = 9.0f * s * pr, p3 = 3.0f * s * pr;
+    const float spr = __fmul_rn(s, P.preff);
+    const float p9 = __fmul_rn(9.0f, spr), p3 = __fmul_rn(3.0f, spr);
     const float om = P.omega;
-    // rest population: h_eq + S = w0 c1
-    if constexpr (W1) h[0] = w3f(0) * c1;
-    else h[0] = fmaf(om, fmaf(w3f(0), c1 + 3.0f * s * pr * uF, -h[0]), h[0]) - w3f(0) * 3.0f * s * pr * uF;
+    const V rho = O::add(O::splat(1.0f), O::mul(drs, O::splat(is)));
+    const V ir = O::recip(rho);
+    ux = O::mul(O::fma(jx, O::splat(is), O::splat(0.5f * Fx)), ir);
+    uy = O::mul(O::fma(jy, O::splat(is), O::splat(0.5f * Fy)), ir);
+    uz = O::mul(O::fma(jz, O::splat(is), O::splat(0.5f * Fz)), ir);
+    const V u2 = O::fma(uz, uz, O::fma(uy, uy, O::mul(ux, ux)));
+    const V uF = O::fma(uz, O::splat(Fz), O::fma(uy, O::splat(Fy), O::mul(ux, O::splat(Fx))));
+    const V srho = O::mul(O::splat(s), rho);
+    // symmetric, eu = eF = 0 part: drs - 1.5 s rho u^2 - 3 s pr uF
+    const V c1 = O::fma(O::splat(-p3), uF, O::fma(O::mul(O::splat(-1.5f), srho), u2, drs));
+    const V r45 = O::mul(O::splat(4.5f), srho), r3 = O::mul(O::splat(3.0f), srho);
+    V c1p, p3uF;
+    if constexpr (W1) {
+        // rest population: h_eq + S = w0 c1
+        h[0] = O::mul(O::splat(w3f(0)), c1);
+    } else {
+        c1p = O::fma(O::splat(p3), uF, c1);      // equilibrium part of c1
+        p3uF = O::mul(O::splat(p3), uF);
+        h[0] = O::sub(O::fma(O::splat(om), O::fma(O::splat(w3f(0)), c1p, O::neg(h[0])), h[0]),
+                      O::mul(O::splat(w3f(0)), p3uF));
+    }
 #pragma unroll
     for (int p = 0; p < 9; ++p) {
         const int k = 2 * p + 1;
         const int cx = ex3(k), cy = ey3(k), cz = ez3(k);
-        float eu = 0.f, eF = 0.f;
-        if (cx) { eu += cx > 0 ? ux : -ux; eF += cx > 0 ? Fx : -Fx; }
-        if (cy) { eu += cy > 0 ? uy : -uy; eF += cy > 0 ? Fy : -Fy; }
-        if (cz) { eu += cz > 0 ? uz : -uz; eF += cz > 0 ? Fz : -Fz; }
+        V eu = O::splat(0.0f);
+        bool fe = true;
+        signed_acc<O>(eu, fe, cx, ux);
+        signed_acc<O>(eu, fe, cy, uy);
+        signed_acc<O>(eu, fe, cz, uz);
+        const float eF = signed_sum3(cx, cy, cz, Fx, Fy, Fz);
         const float w = w3f(k);
+        const float p9eF = __fmul_rn(p9, eF), p3eF = __fmul_rn(p3, eF);
         if constexpr (W1) {
             // (h_eq + S)_k = sym + anti, (h_eq + S)_opp = sym - anti
-            const float sym = w * fmaf(fmaf(r45, eu, p9 * eF), eu, c1);
-            const float anti = w * fmaf(r3, eu, p3 * eF);
-            h[k] = sym + anti;
-            h[k + 1] = sym - anti;
+            const V sym = O::mul(O::splat(w), O::fma(O::fma(r45, eu, O::splat(p9eF)), eu, c1));
+            const V anti = O::mul(O::splat(w), O::fma(r3, eu, O::splat(p3eF)));
+            h[k] = O::add(sym, anti);
+            h[k + 1] = O::sub(sym, anti);
         } else {
             // equilibrium and source split: E = Es +- Ea, S = Ss +- Sa
-            const float Es = w * fmaf(r45 * eu, eu, c1 + 3.0f * s * pr * uF);
-            const float Ea = w * r3 * eu;
-            const float Ss = w * fmaf(p9 * eF, eu, -3.0f * s * pr * uF);
-            const float Sa = w * p3 * eF;
-            h[k] = fmaf(om, (Es + Ea) - h[k], h[k]) + (Ss + Sa);
-            h[k + 1] = fmaf(om, (Es - Ea) - h[k + 1], h[k + 1]) + (Ss - Sa);
+            const V Es = O::mul(O::splat(w), O::fma(O::mul(r45, eu), eu, c1p));
+            const V Ea = O::mul(O::mul(O::splat(w), r3), eu);
+            const V Ss = O::mul(O::splat(w), O::fma(O::splat(p9eF), eu, O::neg(p3uF)));
+            const V Sa = O::splat(__fmul_rn(w, p3eF));
+            h[k] = O::add(O::fma(O::splat(om), O::sub(O::add(Es, Ea), h[k]), h[k]), O::add(Ss, Sa));
+            h[k + 1] = O::add(O::fma(O::splat(om), O::sub(O::sub(Es, Ea), h[k + 1]), h[k + 1]), O::sub(Ss, Sa));
         }
     }
 }
@@ -210,6 +271,12 @@ struct StoreF32 {
     __device__ static __forceinline__ void ld2(const T *p, C &lo, C &hi)
     {
         const float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
+        lo = v.x; hi = v.y;
+    }
+    // the same pair from a shared-memory copy of the slots
+    __device__ static __forceinline__ void lds2(const T *p, C &lo, C &hi)
+    {
+        const float2 v = *reinterpret_cast<const float2 *>(p);
         lo = v.x; hi = v.y;
     }
     __device__ static __forceinline__ void st2(T *p, C lo, C hi, uint32_t, uint32_t)
@@ -252,6 +319,12 @@ struct StoreF16 {
         lo = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
         hi = __half2float(__ushort_as_half((unsigned short)(w >> 16)));
     }
+    __device__ static __forceinline__ void lds2(const T *p, C &lo, C &hi)
+    {
+        const uint32_t w = *reinterpret_cast<const unsigned int *>(p);
+        lo = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+        hi = __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+    }
     __device__ static __forceinline__ void st2(T *p, C lo, C hi, uint32_t rlo, uint32_t rhi)
     {
         const uint32_t rb = (__funnelshift_l(rhi, rhi, 16) << 16) | (__funnelshift_l(rlo, rlo, 16) & 0xffffu);
@@ -286,6 +359,12 @@ struct StoreBF16 {
     __device__ static __forceinline__ void ld2(const T *p, C &lo, C &hi)
     {
         const uint32_t w = __ldcs(reinterpret_cast<const unsigned int *>(p));
+        lo = __bfloat162float(__ushort_as_bfloat16((unsigned short)(w & 0xffffu)));
+        hi = __bfloat162float(__ushort_as_bfloat16((unsigned short)(w >> 16)));
+    }
+    __device__ static __forceinline__ void lds2(const T *p, C &lo, C &hi)
+    {
+        const uint32_t w = *reinterpret_cast<const unsigned int *>(p);
         lo = __bfloat162float(__ushort_as_bfloat16((unsigned short)(w & 0xffffu)));
         hi = __bfloat162float(__ushort_as_bfloat16((unsigned short)(w >> 16)));
     }

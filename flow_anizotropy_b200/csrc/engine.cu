@@ -113,6 +113,7 @@ extern "C" int lbm_create(lbm_ctx **out, int device)
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = prepare_step3d_lp(device);
     if (e != cudaSuccess) {
         lbm_last_error_global() = std::string("CUDA error: ") + cudaGetErrorString(e);
         delete ctx;

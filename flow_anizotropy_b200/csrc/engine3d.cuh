@@ -34,6 +34,7 @@
 #include <stdint.h>
 
 #include "d3q19.cuh"
+#include "tma.cuh"
 
 namespace lbm {
 
@@ -74,6 +75,11 @@ struct Ctl3 {
 };
 
 enum { PH_RUN = 1, PH_AVG = 2, PH_DONE = 3, PH_ERR = 4 };
+
+// Every wait of a step kernel on its own asynchronous copies is bounded by
+// WAIT_NS; a kernel that gives up marks the solve with this status and PH_ERR.
+constexpr int STATUS_WAIT_TIMEOUT = 5;
+constexpr unsigned long long WAIT_NS = 1000000000ull;
 
 // Mutable per-solve state, device resident, written only by the controller.
 struct State3 {
@@ -234,8 +240,17 @@ __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const
     }
 }
 
+// Barrier over the first NT threads of the block: __syncthreads (BAR 0), or
+// the named barrier BAR when other warps of the block do other work.
+template <int NT, int BAR>
+__device__ __forceinline__ void cta_sync()
+{
+    if constexpr (BAR == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(NT) : "memory");
+}
+
 // Block-wide fixed-order sum of three doubles; result valid in thread 0.
-template <int NT = TPB>
+template <int NT = TPB, int BAR = 0>
 __device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
 {
 #pragma unroll
@@ -244,25 +259,25 @@ __device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) { sh[wid][0] = v[0]; sh[wid][1] = v[1]; sh[wid][2] = v[2]; }
-    __syncthreads();
+    cta_sync<NT, BAR>();
     if (threadIdx.x == 0) {
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
         for (int w = 0; w < NT / 32; ++w) { a0 += sh[w][0]; a1 += sh[w][1]; a2 += sh[w][2]; }
         v[0] = a0; v[1] = a1; v[2] = a2;
     }
-    __syncthreads();
+    cta_sync<NT, BAR>();
 }
 
 // Tile finished on a reduction step: publish the tile's flux partial; the
 // last tile of the solve to finish sums all partials in a fixed order (the
 // result does not depend on which blocks ran which tiles, or on what else is
 // in the batch) and runs the controller.
-template <int NT = TPB>
+template <int NT = TPB, int BAR = 0>
 __device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long n,
                                             double (&acc)[3], double (*sh)[3])
 {
     __shared__ int s_last;
-    block_sum3<NT>(acc, sh);
+    block_sum3<NT, BAR>(acc, sh);
     if (threadIdx.x == 0) {
         double *p = S.partials + 3ll * tile;
         p[0] = acc[0]; p[1] = acc[1]; p[2] = acc[2];
@@ -270,7 +285,7 @@ __device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long
         const unsigned prev = atomicAdd(&S.st->counter, 1u);
         s_last = (prev == (unsigned)S.ntiles - 1u);
     }
-    __syncthreads();
+    cta_sync<NT, BAR>();
     if (!s_last) return;
     __threadfence();
     double v[3] = {0.0, 0.0, 0.0};
@@ -279,7 +294,7 @@ __device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long
         v[1] += __ldcg(S.partials + 3ll * t + 1);
         v[2] += __ldcg(S.partials + 3ll * t + 2);
     }
-    block_sum3<NT>(v, sh);
+    block_sum3<NT, BAR>(v, sh);
     if (threadIdx.x == 0) {
         State3 &st = *S.st;
         st.counter = 0u;
@@ -420,12 +435,13 @@ __device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, const uin
 // (NVAR_EVEN_LP for the reduced-precision storage, which adds the grouped
 // even kernels); lbm_tune3d times them on the actual structure.
 struct Variant { int npt, minb; };
-constexpr int NVAR_ODD = 3, NVAR_ODD_LP = 4, NVAR_EVEN = 6, NVAR_EVEN_LP = 8;
+constexpr int NVAR_ODD = 3, NVAR_ODD_LP = 5, NVAR_EVEN = 6, NVAR_EVEN_LP = 8;
 constexpr int NVAR_LP = NVAR_ODD_LP * NVAR_EVEN_LP, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
 constexpr int MAX_GROUP = 3;    // directions per grouped even step
 inline int nvar_even(int prec) { return prec == 0 ? NVAR_EVEN : NVAR_EVEN_LP; }
 // odd variants: 0-1 one voxel per thread, 2 two voxels a tile-half apart, 3
-// two adjacent voxels per thread with paired (vector) slot accesses
+// two adjacent voxels per thread with paired (vector) slot accesses, 4 the
+// same collision fed from a shared-memory ring filled by bulk copies
 __host__ __device__ constexpr Variant odd_lp(int v)
 {
     return v == 0 ? Variant{1, 4} : v == 1 ? Variant{1, 5} : Variant{2, 2};
@@ -490,8 +506,17 @@ __device__ __forceinline__ uint32_t voxel_bits(unsigned i, long long n)
 template <class ST, bool W1, class Cp>
 __device__ __forceinline__ void collide3(Cp (&g)[Q3], const Solve3 &S, Cp &ux, Cp &uy, Cp &uz)
 {
-    if constexpr (ST::shifted) collide_pairs<W1>(g, S.P, S.scale, S.inv_scale, ux, uy, uz);
+    if constexpr (ST::shifted) collide_pairs<W1, F32x1>(g, S.P, S.scale, S.inv_scale, ux, uy, uz);
     else collide_ref64(g, S.P, ux, uy, uz);
+}
+
+// Two voxels' populations collided together (packed FP32, the same bits per
+// voxel as collide3 on each); u receives both velocities.
+template <class ST, bool W1>
+__device__ __forceinline__ void collide3x2(float2 (&g)[Q3], const Solve3 &S, float2 (&u)[3])
+{
+    static_assert(ST::shifted, "the packed operator is the reduced-precision one");
+    collide_pairs<W1, F32x2>(g, S.P, S.scale, S.inv_scale, u[0], u[1], u[2]);
 }
 
 // Odd (local) step: read A[k][i], collide, write A[opp k][i].  The NPT voxels
@@ -527,17 +552,37 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
 #pragma unroll
                 for (int k = 0; k < Q3; ++k) g[j][k] = vv[j] ? ST::ld(A + (k * P + iv[j])) : Cp(0);
             }
+            if constexpr (NPT == 2 && ST::shifted) {
+                // both voxels collide together (packed); an invalid one
+                // computes on zeros and is neither stored nor summed
+                float2 gp[Q3], u[3];
 #pragma unroll
-            for (int j = 0; j < NPT; ++j) {
-                if (!vv[j]) continue;
-                Cp ux, uy, uz;
-                collide3<ST, W1>(g[j], S, ux, uy, uz);
-                {
+                for (int k = 0; k < Q3; ++k) gp[k] = make_float2(g[0][k], g[1][k]);
+                collide3x2<ST, W1>(gp, S, u);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    if (!vv[j]) continue;
                     const uint32_t hv = voxel_bits<ST>(iv[j], n);
 #pragma unroll
-                    for (int k = 0; k < Q3; ++k) store_pop<ST>(A, opp3(k) * P + iv[j], g[j][k], hv, k);
+                    for (int k = 0; k < Q3; ++k)
+                        store_pop<ST>(A, opp3(k) * P + iv[j], j ? gp[k].y : gp[k].x, hv, k);
+                    acc[0] += (double)(j ? u[0].y : u[0].x);
+                    acc[1] += (double)(j ? u[1].y : u[1].x);
+                    acc[2] += (double)(j ? u[2].y : u[2].x);
                 }
-                acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+            } else {
+#pragma unroll
+                for (int j = 0; j < NPT; ++j) {
+                    if (!vv[j]) continue;
+                    Cp ux, uy, uz;
+                    collide3<ST, W1>(g[j], S, ux, uy, uz);
+                    {
+                        const uint32_t hv = voxel_bits<ST>(iv[j], n);
+#pragma unroll
+                        for (int k = 0; k < Q3; ++k) store_pop<ST>(A, opp3(k) * P + iv[j], g[j][k], hv, k);
+                    }
+                    acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+                }
             }
         }
         if (red) finish_tile(S, item.y, n, acc, sh);
@@ -546,16 +591,16 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
 
 // Odd (local) step with two adjacent pore voxels (i, i + 1), i even, per
 // thread: every slot pair of a plane is one aligned 8-byte (FP32) or 4-byte
-// (16-bit) access, and the 16-bit types round both values with one cvt.rs
-// fed with the bits each would get alone, so the populations equal those of
-// step3d_odd_kernel (the flux partials are summed in another order).  The
+// (16-bit) access, the two voxels collide together in packed FP32, and the
+// 16-bit types round both values with one cvt.rs fed with the bits each would
+// get alone, so the populations equal those of step3d_odd_kernel (the flux
+// partials are summed in another order).  The
 // partner of the last voxel of an odd-sized lattice is a padding slot (the
 // plane stride is a multiple of 64); it is read and written but never used.
 template <class ST, int MINB, bool W1>
 __global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepArgs a)
 {
     using T = typename ST::T;
-    using Cp = typename ST::C;
     static_assert(TILE_NPT == 2, "a tile is one voxel pair per thread");
     __shared__ double sh[TPB / 32][3];
     const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
@@ -572,20 +617,178 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepAr
         const unsigned i0 = (unsigned)(item.y * (TPB * TILE_NPT) + 2 * threadIdx.x);
         if (i0 < (unsigned)S.nfluid) {
             const bool v1 = i0 + 1u < (unsigned)S.nfluid;
-            Cp g0[Q3], g1[Q3];
+            float2 g[Q3], u[3];
 #pragma unroll
-            for (int k = 0; k < Q3; ++k) ST::ld2(A + (k * P + i0), g0[k], g1[k]);
-            Cp ux0, uy0, uz0, ux1 = Cp(0), uy1 = Cp(0), uz1 = Cp(0);
-            collide3<ST, W1>(g0, S, ux0, uy0, uz0);
-            if (v1) collide3<ST, W1>(g1, S, ux1, uy1, uz1);
+            for (int k = 0; k < Q3; ++k) ST::ld2(A + (k * P + i0), g[k].x, g[k].y);
+            collide3x2<ST, W1>(g, S, u);
             const uint32_t h0 = voxel_bits<ST>(i0, n), h1 = voxel_bits<ST>(i0 + 1u, n);
 #pragma unroll
             for (int k = 0; k < Q3; ++k)
-                ST::st2(A + (opp3(k) * P + i0), g0[k], g1[k], dir_bits(h0, k), dir_bits(h1, k));
-            acc[0] += (double)ux0; acc[1] += (double)uy0; acc[2] += (double)uz0;
-            if (v1) { acc[0] += (double)ux1; acc[1] += (double)uy1; acc[2] += (double)uz1; }
+                ST::st2(A + (opp3(k) * P + i0), g[k].x, g[k].y, dir_bits(h0, k), dir_bits(h1, k));
+            acc[0] += (double)u[0].x; acc[1] += (double)u[1].x; acc[2] += (double)u[2].x;
+            if (v1) { acc[0] += (double)u[0].y; acc[1] += (double)u[1].y; acc[2] += (double)u[2].y; }
         }
         if (red) finish_tile(S, item.y, n, acc, sh);
+    }
+}
+
+// Odd (local) step staged through shared memory by the copy engine.  A
+// producer warp (the block's last 32 threads; one lane works) walks the work
+// list (persistent grid, stride gridDim.x), skips items of finished solves,
+// and for each tile (TPB * TILE_NPT voxels) issues 19 untiled bulk copies,
+// one per plane run, into a ring of ODD_BULK_STAGES tile buffers; each
+// buffer carries its item index.  The TPB consumer threads collide a tile
+// out of shared memory (two adjacent voxels per thread, packed, as the pair
+// kernel), store it straight to global memory and release the buffer.  So
+// the loads of the next tiles are in flight while a tile is collided, and
+// the producer's work-list reads never stall the consumers.  Populations and
+// fluxes equal those of step3d_odd_pair_kernel bit for bit.  Every wait is
+// bounded: consumers that give up mark the solve and leave, and the producer
+// waits (bounded) for its copies in flight before it returns.
+constexpr int ODD_BULK_STAGES_16 = 4, ODD_BULK_STAGES_32 = 2;
+constexpr int ODD_BULK_THREADS = TPB + 32;
+template <class T>
+__host__ __device__ constexpr int odd_bulk_stages() { return sizeof(T) == 4 ? ODD_BULK_STAGES_32 : ODD_BULK_STAGES_16; }
+template <class T>
+__host__ __device__ constexpr unsigned odd_bulk_smem()
+{
+    return (unsigned)odd_bulk_stages<T>() * Q3 * TPB * TILE_NPT * (unsigned)sizeof(T);
+}
+
+template <class ST, int MINB, bool W1>
+__global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    static_assert(TILE_NPT == 2, "a tile is one voxel pair per thread");
+    constexpr int NS = odd_bulk_stages<T>();
+    constexpr unsigned TV = TPB * TILE_NPT;              // voxels of a tile
+    constexpr unsigned RUN = TV * (unsigned)sizeof(T);   // bytes of one plane run
+    constexpr int BAR = 1;                               // consumers' named barrier
+    extern __shared__ __align__(128) unsigned char ring[];
+    __shared__ uint64_t full[NS], empty[NS];
+    __shared__ int slot_item[NS];
+    __shared__ double sh[TPB / 32][3];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1u);
+            mbar_init(&empty[s], (unsigned)TPB);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+
+    if (tid >= TPB) {
+        // ------------------------------------------------------ producer --
+        if (tid != TPB) return;
+        int next = blockIdx.x;
+        unsigned eparity = 0u, fparity = 0u, copies = 0u;   // copies: buffers with bytes issued
+        for (int t = 0;; ++t) {
+            const int s = t % NS;
+            if (t >= NS) {
+                // the consumers' release of this buffer's previous tile
+                if (!mbar_wait_bounded(&empty[s], (eparity >> s) & 1u, WAIT_NS)) break;
+                eparity ^= 1u << s;
+                copies &= ~(1u << s);
+            }
+            int w = next;
+            unsigned bytes = 0u, P = 0u;
+            const T *src = nullptr;
+            for (; w < nwork; w += gridDim.x) {
+                const int2 it = a.work[w];
+                const Solve3 &S = a.solves[it.x];
+                if (S.st->phase >= PH_DONE) continue;
+                const unsigned i0 = (unsigned)it.y * TV;
+                src = static_cast<const T *>(S.A) + i0;
+                P = (unsigned)S.plane;
+                if ((reinterpret_cast<uintptr_t>(src) | (uintptr_t)P * sizeof(T)) & 15u) {
+                    // not a legal bulk copy (lattices are allocated aligned
+                    // and planes padded to 64 slots, so this does not happen):
+                    // the solve is failed instead of copied
+                    S.st->status = STATUS_WAIT_TIMEOUT;
+                    S.st->phase = PH_ERR;
+                    continue;
+                }
+                bytes = ((unsigned)min(TV, (unsigned)S.nfluid - i0) * (unsigned)sizeof(T) + 15u) & ~15u;
+                break;
+            }
+            const bool more = w < nwork;
+            next = more ? w + gridDim.x : w;
+            slot_item[s] = more ? w : -1;
+            if (more && bytes) {
+                unsigned char *buf = ring + s * (Q3 * RUN);
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&full[s], Q3 * bytes);
+#pragma unroll 1
+                for (int k = 0; k < Q3; ++k) bulk_load(buf + k * RUN, src + (size_t)k * P, bytes, &full[s]);
+                copies |= 1u << s;
+            } else {
+                mbar_arrive(&full[s]);   // end of the list, or an item without voxels
+            }
+            fparity ^= 1u << s;
+            if (!more) return;           // the consumers stop at this buffer
+        }
+        // gave up on a release: wait for the copies still in flight, then leave
+        for (int r = 0; r < NS; ++r)
+            if ((copies >> r) & 1u) mbar_wait_bounded(&full[r], ((fparity >> r) & 1u) ^ 1u, WAIT_NS);
+        return;
+    }
+
+    // -------------------------------------------------------- consumers --
+    unsigned parity = 0u;
+    for (int t = 0;; ++t) {
+        const int s = t % NS;
+        const bool ok = mbar_wait_bounded(&full[s], (parity >> s) & 1u, WAIT_NS);
+        int bad;
+        asm volatile("{\n\t.reg .pred p, q;\n\t"
+                     "setp.ne.u32 p, %1, 0;\n\t"
+                     "bar.red.or.pred q, %2, %3, p;\n\t"
+                     "selp.u32 %0, 1, 0, q;\n\t}"
+                     : "=r"(bad)
+                     : "r"((unsigned)!ok), "n"(BAR), "n"(TPB)
+                     : "memory");
+        if (bad) {
+            if (tid == 0) {
+                // the item index is written before the buffer's copies are
+                // issued, so it is there even if they never completed
+                const int w = *static_cast<volatile int *>(&slot_item[s]);
+                if (w >= 0) {
+                    const Solve3 &S = a.solves[a.work[w].x];
+                    S.st->status = STATUS_WAIT_TIMEOUT;
+                    S.st->phase = PH_ERR;
+                    __threadfence();
+                }
+            }
+            return;
+        }
+        parity ^= 1u << s;
+        const int w = slot_item[s];
+        if (w < 0) break;
+        const int2 item = a.work[w];
+        const Solve3 &S = a.solves[item.x];
+        const long long n = S.st->s_base + a.step + 1;
+        const bool red = needs_reduction(S.c, S.st->phase, n);
+        T *__restrict__ A = static_cast<T *>(S.A);
+        const unsigned P = (unsigned)S.plane;
+        const T *buf = reinterpret_cast<const T *>(ring + s * (Q3 * RUN));
+        double acc[3] = {0.0, 0.0, 0.0};
+        const unsigned i0 = (unsigned)item.y * TV + 2u * tid;
+        float2 g[Q3], u[3];
+#pragma unroll
+        for (int k = 0; k < Q3; ++k) ST::lds2(buf + (k * TV + 2u * tid), g[k].x, g[k].y);
+        mbar_arrive(&empty[s]);    // this thread is done with buffer s
+        if (i0 < (unsigned)S.nfluid) {
+            const bool v1 = i0 + 1u < (unsigned)S.nfluid;
+            collide3x2<ST, W1>(g, S, u);
+            const uint32_t h0 = voxel_bits<ST>(i0, n), h1 = voxel_bits<ST>(i0 + 1u, n);
+#pragma unroll
+            for (int k = 0; k < Q3; ++k)
+                ST::st2(A + (opp3(k) * P + i0), g[k].x, g[k].y, dir_bits(h0, k), dir_bits(h1, k));
+            acc[0] += (double)u[0].x; acc[1] += (double)u[1].x; acc[2] += (double)u[2].x;
+            if (v1) { acc[0] += (double)u[0].y; acc[1] += (double)u[1].y; acc[2] += (double)u[2].y; }
+        }
+        if (red) finish_tile<TPB, BAR>(S, item.y, n, acc, sh);
     }
 }
 
@@ -909,6 +1112,9 @@ __global__ void canon3d_kernel(const Solve3 S, long long done, double *f_out, fl
 cudaError_t launch_step3d_f64(int variant, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a);
 cudaError_t launch_step3d_lp(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a);
 cudaError_t launch_init3d(int prec, void *A, long long plane, long long n, cudaStream_t s);
+// Allow the bulk-staged odd kernels their shared-memory ring on device `dev`
+// (once per device, before any launch or capture).
+cudaError_t prepare_step3d_lp(int dev);
 cudaError_t launch_canon3d(int prec, const Solve3 &S, long long done, double *f, float *u, cudaStream_t s);
 int max_blocks_step3d(int prec, int variant, bool odd);
 inline bool is_moment(int prec) { return prec == 4 || prec == 5; }

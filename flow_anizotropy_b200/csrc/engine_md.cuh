@@ -51,8 +51,8 @@ constexpr int MD_MASK_BYTES = MD_MX * MD_HY;
 constexpr int MD_SLOT = (MD_MASK_OFF + MD_MASK_BYTES + 127) / 128 * 128;
 constexpr unsigned MD_TX = MD_REC_BYTES + MD_MASK_BYTES;    // bytes per plane (both loads)
 constexpr int MD_MAPS_BYTES = 512;                          // tensor maps at the head of a lattice
-constexpr unsigned long long MD_WAIT_NS = 1000000000ull;
-constexpr int MD_STATUS_TIMEOUT = 5;
+constexpr unsigned long long MD_WAIT_NS = WAIT_NS;
+constexpr int MD_STATUS_TIMEOUT = STATUS_WAIT_TIMEOUT;
 
 // ring depth and register budget per variant (z-segment length: md_lz)
 __host__ __device__ constexpr int md_ns(int v) { return v == 3 ? 6 : 4; }

@@ -1,5 +1,7 @@
 // Reduced-precision D3Q19 kernels: shifted populations stored as FP32, FP16
 // (power-of-two scaled) or BF16, collision in FP32, flux reduced in FP64.
+#include <algorithm>
+
 #include "engine3d.cuh"
 
 namespace lbm {
@@ -13,6 +15,46 @@ int max_blocks_f64(int variant, bool odd);
 #define LBM_EVEN(ST, V, W) step3d_even_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 #define LBM_EVENA(ST, V, W) step3d_even_async_kernel<ST, even_lp(V).minb, W>
 #define LBM_EVENG(ST, V, W) step3d_even_group_kernel<ST, even_lp(V).minb, W, even_meta(V)>
+#define LBM_ODDB(ST, W) step3d_odd_bulk_kernel<ST, odd_lp(4).minb, W>
+
+// Persistent CTAs of the bulk-staged odd kernel per (storage, tau = 1, device),
+// set by prepare_bulk once its shared-memory ring has been allowed.
+static int g_bulk_ctas[3][2][64];
+
+template <class ST, bool W>
+static int prepare_bulk(int dev)
+{
+    using T = typename ST::T;
+    const void *k = (const void *)LBM_ODDB(ST, W);
+    const unsigned smem = odd_bulk_smem<T>();
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    int nb = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, ODD_BULK_THREADS, smem) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    g_bulk_ctas[ST::code - 1][W ? 1 : 0][dev] = nb * sms;
+    return nb;
+}
+
+cudaError_t prepare_step3d_lp(int dev)
+{
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    const bool ok = prepare_bulk<StoreF32, true>(dev) > 0 && prepare_bulk<StoreF32, false>(dev) > 0
+                 && prepare_bulk<StoreF16, true>(dev) > 0 && prepare_bulk<StoreF16, false>(dev) > 0
+                 && prepare_bulk<StoreBF16, true>(dev) > 0 && prepare_bulk<StoreBF16, false>(dev) > 0;
+    return ok ? cudaSuccess : cudaErrorInvalidConfiguration;
+}
+
+template <class ST, bool W>
+static cudaError_t launch_bulk(dim3 grid, cudaStream_t s, const StepArgs &a)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int ctas = (dev >= 0 && dev < 64) ? g_bulk_ctas[ST::code - 1][W ? 1 : 0][dev] : 0;
+    if (ctas <= 0) return cudaErrorInvalidConfiguration;   // prepare_step3d_lp not run on this device
+    grid.x = std::min<unsigned>(grid.x, (unsigned)ctas);
+    LBM_ODDB(ST, W)<<<grid, ODD_BULK_THREADS, odd_bulk_smem<typename ST::T>(), s>>>(a);
+    return cudaSuccess;
+}
 
 template <class ST, bool W>
 static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
@@ -24,7 +66,11 @@ static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const S
         case 0: LBM_ODD(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
         case 1: LBM_ODD(ST, 1, W)<<<grid, TPB, 0, s>>>(a); break;
         case 2: LBM_ODD(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_ODDP(ST, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 3: LBM_ODDP(ST, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: {
+            const cudaError_t e = launch_bulk<ST, W>(grid, s, a);
+            if (e != cudaSuccess) return e;
+        } break;
         }
     } else {
         switch (ve) {
@@ -55,6 +101,11 @@ template <class ST>
 static int occ(int v, bool odd)
 {
     const int vo = v / NVAR_EVEN_LP, ve = v % NVAR_EVEN_LP;
+    if (odd && vo == 4) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        return prepare_bulk<ST, true>(dev);
+    }
     const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(ST, 0, true) : vo == 1 ? (const void *)LBM_ODD(ST, 1, true)
                            : vo == 2 ? (const void *)LBM_ODD(ST, 2, true) : (const void *)LBM_ODDP(ST, true))
                         : (ve == 0 ? (const void *)LBM_EVEN(ST, 0, true) : ve == 1 ? (const void *)LBM_EVEN(ST, 1, true)

@@ -1,6 +1,7 @@
 // Tensor-memory-accelerator (TMA) copies and shared-memory barriers for
-// sm_100a, as inline PTX.  Only plain (non-multicast) tiled loads from this
-// GPU's own global memory into the issuing CTA's shared memory are used.
+// sm_100a, as inline PTX.  Only plain (non-multicast) tiled and untiled bulk
+// loads from this GPU's own global memory into the issuing CTA's shared
+// memory are used.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -41,6 +42,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned by
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
+}
+
+// Plain arrival (no transaction bytes): completes a phase that carries no copy.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
@@ -95,6 +102,16 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const void *tmap, int c0,
         " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
         "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
         : "memory");
+}
+
+// Untiled bulk copy of `bytes` from global to this CTA's shared memory,
+// completing on `bar`: both addresses 16-byte aligned, `bytes` a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 }  // namespace lbm

@@ -91,4 +91,4 @@ def test_grouped_even_step_equals_per_direction(gpu, packing, prec, ndir):
             assert a.steps == b.steps and a.converged == b.converged
             assert np.array_equal(a.q, b.q) and np.array_equal(a.se, b.se), ve
         assert np.array_equal(vel, vel0), ve
-    assert S.variant_count(prec) == 4 * nv_even
+    assert S.variant_count(prec) == 5 * nv_even
