@@ -26,7 +26,7 @@ SYMBOLS = (
     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_bytes3d", "lbm_batch_submit3d",
     "lbm_batch_run", "lbm_batch_poll", "lbm_batch_active", "lbm_batch_resident_bytes",
     "lbm_variant_count", "lbm_tune3d",
-    "lbm_debug_steps3d", "lbm_debug_steps2d",
+    "lbm_debug_steps3d", "lbm_debug_steps2d", "lbm_debug_bulk_wait",
     "lbm_trig_structure3d", "lbm_percolates3d",
 )
 
@@ -125,6 +125,8 @@ def load(path: Path | str | None = None):
         L.lbm_tune3d.argtypes = [vp, u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                  dp, C.POINTER(C.c_int)]
         L.lbm_tune3d.restype = C.c_int
+        L.lbm_debug_bulk_wait.argtypes = [vp, C.c_ulonglong, C.c_int]
+        L.lbm_debug_bulk_wait.restype = C.c_int
         L.lbm_debug_steps3d.argtypes = [vp, u8p, C.c_int, C.c_int, C.c_int, dp, C.c_double,
                                         C.c_int, C.c_int, C.c_longlong, dp, fp, dp]
         L.lbm_debug_steps3d.restype = C.c_int

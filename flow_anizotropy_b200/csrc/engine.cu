@@ -396,6 +396,10 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
         cudaGraph_t &g; cudaGraphExec_t &e;
         ~GraphGuard() { if (e) cudaGraphExecDestroy(e); if (g) cudaGraphDestroy(g); }
     } guard{graph, exec};
+    a.wait_ns = ctx->test_wait_ns;
+    a.starve = ctx->test_starve;
+    ae.wait_ns = a.wait_ns;
+    ae.starve = a.starve;
     auto launch = [&](long long rel, bool odd) {
         StepArgs x = odd ? a : ae;
         x.step = rel;
@@ -537,7 +541,10 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
         r.steps = st.steps;
         r.converged = st.converged;
         r.status = st.status;
-        if (st.status) {
+        if (st.status == STATUS_WAIT_TIMEOUT) {
+            ctx->err = "run " + std::to_string(j) + ": a step kernel gave up waiting for its shared-memory copies";
+            out = LBM_ECUDA;
+        } else if (st.status) {
             ctx->err = "non-finite flux in run " + std::to_string(j) + " at step " + std::to_string(st.steps);
             out = LBM_EINPUT;
         } else if (!st.converged && out == LBM_OK) {
@@ -546,6 +553,14 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
     }
     CK(cudaStreamSynchronize(ctx->stream));
     return out;
+}
+
+extern "C" int lbm_debug_bulk_wait(lbm_ctx *ctx, unsigned long long wait_ns, int starve)
+{
+    if (!ctx) return LBM_EINPUT;
+    ctx->test_wait_ns = wait_ns;
+    ctx->test_starve = starve ? 1 : 0;
+    return LBM_OK;
 }
 
 extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz,

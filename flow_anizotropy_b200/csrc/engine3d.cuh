@@ -138,6 +138,8 @@ struct StepArgs {
     const int *nwork_dev; // if non-null, the item count is read here
     int nwork;
     long long step;       // steps completed = st->s_base + step
+    unsigned long long wait_ns = 0;   // bulk-staged kernels: wait limit (0: WAIT_NS)
+    int starve = 0;                   // test only: the bulk producer issues nothing
 };
 
 // ----------------------------------------------------------------- helpers --
@@ -670,10 +672,12 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
     __shared__ double sh[TPB / 32][3];
     const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
     const int tid = threadIdx.x;
+    const unsigned long long wait_ns = a.wait_ns ? a.wait_ns : WAIT_NS;
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
             mbar_init(&full[s], 1u);
             mbar_init(&empty[s], (unsigned)TPB);
+            slot_item[s] = -1;
         }
         mbar_init_fence();
     }
@@ -681,14 +685,14 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
 
     if (tid >= TPB) {
         // ------------------------------------------------------ producer --
-        if (tid != TPB) return;
+        if (tid != TPB || a.starve) return;
         int next = blockIdx.x;
         unsigned eparity = 0u, fparity = 0u, copies = 0u;   // copies: buffers with bytes issued
         for (int t = 0;; ++t) {
             const int s = t % NS;
             if (t >= NS) {
                 // the consumers' release of this buffer's previous tile
-                if (!mbar_wait_bounded(&empty[s], (eparity >> s) & 1u, WAIT_NS)) break;
+                if (!mbar_wait_bounded(&empty[s], (eparity >> s) & 1u, wait_ns)) break;
                 eparity ^= 1u << s;
                 copies &= ~(1u << s);
             }
@@ -731,7 +735,7 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
         }
         // gave up on a release: wait for the copies still in flight, then leave
         for (int r = 0; r < NS; ++r)
-            if ((copies >> r) & 1u) mbar_wait_bounded(&full[r], ((fparity >> r) & 1u) ^ 1u, WAIT_NS);
+            if ((copies >> r) & 1u) mbar_wait_bounded(&full[r], ((fparity >> r) & 1u) ^ 1u, wait_ns);
         return;
     }
 
@@ -739,7 +743,7 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
     unsigned parity = 0u;
     for (int t = 0;; ++t) {
         const int s = t % NS;
-        const bool ok = mbar_wait_bounded(&full[s], (parity >> s) & 1u, WAIT_NS);
+        const bool ok = mbar_wait_bounded(&full[s], (parity >> s) & 1u, wait_ns);
         int bad;
         asm volatile("{\n\t.reg .pred p, q;\n\t"
                      "setp.ne.u32 p, %1, 0;\n\t"
@@ -751,8 +755,10 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
         if (bad) {
             if (tid == 0) {
                 // the item index is written before the buffer's copies are
-                // issued, so it is there even if they never completed
-                const int w = *static_cast<volatile int *>(&slot_item[s]);
+                // issued, so it is there even if they never completed; with
+                // none, the CTA's first item names the solve
+                int w = *static_cast<volatile int *>(&slot_item[s]);
+                if (w < 0 && (int)blockIdx.x < nwork) w = blockIdx.x;
                 if (w >= 0) {
                     const Solve3 &S = a.solves[a.work[w].x];
                     S.st->status = STATUS_WAIT_TIMEOUT;

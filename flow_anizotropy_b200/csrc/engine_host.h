@@ -13,6 +13,10 @@ struct lbm_ctx {
     cudaStream_t stream = nullptr;
     int sms = 0;
     std::string err;
+    // test knobs of the bulk-staged odd step (lbm_debug_bulk_wait): wait
+    // limit in ns (0: the kernels' own), and a producer that issues nothing
+    unsigned long long test_wait_ns = 0;
+    int test_starve = 0;
 };
 
 int lbm_fail_cuda(lbm_ctx *ctx, cudaError_t e, const char *what, int line);

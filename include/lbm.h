@@ -87,7 +87,7 @@ typedef struct {
     double    se[3];        /* standard error over the averaging phase        */
     long long steps;
     int       converged;
-    int       status;       /* LBM_OK or LBM_EINPUT (non-finite flux)         */
+    int       status;       /* 0; 2 non-finite flux; 5 a copy wait ran out    */
 } lbm_result3d;
 
 /* D2Q9 knobs of LMB2d/main.cpp:64-79 plus tau (LMB2d/lbm.cpp:86). */
@@ -250,6 +250,13 @@ int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz, int n
 int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int nz,
                       const double force[3], double tau, int precision, int variant,
                       long long nsteps, double *f_out, float *u_out, double q_out[3]);
+
+/* Test knobs of the bulk-staged odd step (odd variant 4) in this context:
+ * wait_ns replaces the 1 s limit of its waits on shared-memory copies (0
+ * restores it), and starve != 0 makes its producer issue nothing, so the
+ * waits run out: the solve then ends with status 5 and the call returns
+ * LBM_ECUDA, the context staying usable.  No counterpart in the reference. */
+int lbm_debug_bulk_wait(lbm_ctx *ctx, unsigned long long wait_ns, int starve);
 
 /* 2D counterpart: populations of the buffer the next step reads, ny x nx x 9
  * floats, the U,V of the last step (ny x nx x 2) and its flux. */

@@ -75,3 +75,26 @@ def test_bulk_odd_whole_solves_identical(gpu, prec):
 def test_variant_table_has_bulk_odd(gpu):
     for prec in ("fp32", "fp16", "bf16"):
         assert S.variant_count(prec) == 5 * NV_EVEN
+
+
+def test_starved_waits_end_with_status(gpu):
+    """Failure path of the bounded waits, with no fault: the producer issues
+    nothing (test knob), the consumers' 2 ms waits run out, the solve ends
+    with status 5 and the call fails with LBM_ECUDA; the context stays usable
+    and the next solve is the normal one."""
+    from flow_anizotropy_b200 import _lib
+    solid = st.sphere_packing((20, 24, 28), 4.0, 0.6, seed=11, percolate=(True, True, True))
+    F = 1e-6
+    prm = dict(eps=1e-7, lag=200, hold=2, min_steps=400, max_steps=6000, avg_steps=100)
+    p = S.Params3D(precision="fp16", variant=_variant(BULK), **prm)
+    gpu.check(gpu.L.lbm_debug_bulk_wait(gpu.h, 2_000_000, 1))
+    try:
+        with pytest.raises(_lib.LBMError) as e:
+            S.solve3d(solid, [[F, 0, 0]], p)
+        assert e.value.code == _lib.LBM_ECUDA
+        assert "gave up waiting" in gpu.error()
+    finally:
+        gpu.check(gpu.L.lbm_debug_bulk_wait(gpu.h, 0, 0))
+    ok, rc, _ = S.solve3d(solid, [[F, 0, 0]], p)
+    ref, rc0, _ = S.solve3d(solid, [[F, 0, 0]], S.Params3D(precision="fp16", variant=_variant(PAIR), **prm))
+    assert rc == rc0 and ok[0].steps == ref[0].steps and np.array_equal(ok[0].q, ref[0].q)
