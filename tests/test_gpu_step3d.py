@@ -72,7 +72,7 @@ def test_shifted_storage(gpu, prec, tol):
         np.testing.assert_allclose(q, qo, rtol=tol * 5)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32", "fp16"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "fp16", "bf16"])
 def test_every_variant_agrees(gpu, prec):
     """Each step-kernel variant (pore voxels per thread x register budget) gives
     the same populations: bit for bit within a precision."""
@@ -91,6 +91,25 @@ def test_every_variant_agrees(gpu, prec):
             else:
                 assert np.array_equal(f, ref[n][0]), (prec, v, n)
                 np.testing.assert_allclose(q, ref[n][1], rtol=1e-12)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16", "bf16"])
+def test_every_odd_variant_agrees_general_tau(gpu, prec):
+    """tau != 1 (the general operator, packed and scalar forms): every odd
+    variant with the same even kernel gives the same populations, bit for
+    bit, after odd and even step counts."""
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200.solver import debug_steps3d
+    solid = _solid((10, 13, 37), 23)
+    force = [-4e-7, 2e-7, 1e-6]
+    nv = _lib.load().lbm_variant_count(_lib.PRECISIONS[prec])
+    nv_even = 8
+    ref = {n: debug_steps3d(solid, force, n, tau=0.8, precision=prec, variant=1) for n in (3, 4)}
+    for vo in range(1, nv // nv_even):
+        for n in (3, 4):
+            f, u, q = debug_steps3d(solid, force, n, tau=0.8, precision=prec, variant=vo * nv_even + 1)
+            assert np.array_equal(f, ref[n][0]) and np.array_equal(u, ref[n][1]), (prec, vo, n)
+            np.testing.assert_allclose(q, ref[n][2], rtol=1e-12)
 
 
 @pytest.mark.parametrize("prec,tol", [("fp32", 2e-6), ("fp16", 2e-3)])
