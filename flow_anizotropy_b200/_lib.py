@@ -14,6 +14,7 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "liblbm.so"
 
 LBM_OK, LBM_EINPUT, LBM_NOT_CONVERGED, LBM_EBUSY, LBM_ECUDA = 0, 2, 3, 4, -1
+LBM_VARIANT_DEFAULT = -1      # the library's per-precision default step-kernel variant
 FP64, FP32, FP16, BF16, M32, M64, MD32 = 0, 1, 2, 3, 4, 5, 6
 PRECISIONS = {"fp64": FP64, "fp32": FP32, "fp16": FP16, "bf16": BF16, "m32": M32, "m64": M64,
               "md32": MD32}

@@ -156,9 +156,24 @@ int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
     if (p.criterion != LBM_CRIT_DRIFT && p.criterion != LBM_CRIT_BLOCK) return lbm_fail_input(ctx, "unknown criterion");
     if (p.criterion == LBM_CRIT_BLOCK && (p.sample <= 0 || p.lag % p.sample != 0))
         return lbm_fail_input(ctx, "block criterion needs sample > 0 dividing lag");
-    if (p.variant < 0 || p.variant >= variant_count(p.precision))
+    if (p.variant != LBM_VARIANT_DEFAULT && (p.variant < 0 || p.variant >= variant_count(p.precision)))
         return lbm_fail_input(ctx, "unknown step-kernel variant");
     return LBM_OK;
+}
+
+// The autotuner's pick on the 128^3 tensor workload: FP32 plain odd + even
+// ranks from the mask; 16-bit bulk-staged odd + even from neighbour records.
+int lbm_default_variant(int prec)
+{
+    if (prec == LBM_FP32) return 0 * NVAR_EVEN_LP + 3;
+    if (prec == LBM_FP16 || prec == LBM_BF16) return 4 * NVAR_EVEN_LP + 1;
+    return 0;
+}
+
+static lbm_params3d lbm_resolve_variant(lbm_params3d p)
+{
+    if (p.variant == LBM_VARIANT_DEFAULT) p.variant = lbm_default_variant(p.precision);
+    return p;
 }
 
 static size_t elem_size(int prec) { return prec == LBM_FP64 ? 8 : (prec == LBM_FP32 ? 4 : 2); }
@@ -468,9 +483,9 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
     const long long nn = (long long)nx * ny * nz;
     if (nn >= (1ll << 31) || (long long)Q3 * lbm_plane_elems(nn) >= (1ll << 32))
         return lbm_fail_input(ctx, "lattice too large (19 x nodes must stay below 2^32)");
-    const lbm_params3d p = *params;
-    int rc = lbm_check_params3d(ctx, p);
+    int rc = lbm_check_params3d(ctx, *params);
     if (rc) return rc;
+    const lbm_params3d p = lbm_resolve_variant(*params);
     const int prec = p.precision, npt = lbm_pick_npt(p);
 
     DevMem mask(ctx->stream);
@@ -580,6 +595,8 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     p.precision = precision; p.criterion = LBM_CRIT_DRIFT; p.variant = variant; p.sample = 1;
     int rc = lbm_check_params3d(ctx, p);
     if (rc) return rc;
+    p = lbm_resolve_variant(p);
+    variant = p.variant;
     const int npt = lbm_pick_npt(p);
     DevMem mask(ctx->stream);
     long long npore = 0;

@@ -591,12 +591,36 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
     }
 }
 
+// Flux partial of a thread in the canonical order of a tile (thread t sums
+// voxel t, then voxel t + TPB, as the one-voxel kernels do), for kernels
+// whose threads own the adjacent voxels (2t, 2t + 1): the velocities are
+// exchanged through shared memory, so every kernel variant reduces the same
+// values in the same order and the fluxes agree bit for bit.  Called by all
+// NT threads of the barrier group on reduction steps.
+template <int NT, int BAR>
+__device__ __forceinline__ void canonical_acc(float (*su)[TPB * TILE_NPT], const float2 (&u)[3], unsigned tid,
+                                              unsigned tile_start, unsigned nfluid, double (&acc)[3])
+{
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        su[c][2 * tid] = u[c].x;
+        su[c][2 * tid + 1] = u[c].y;
+    }
+    cta_sync<NT, BAR>();
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        acc[c] = 0.0;
+        if (tile_start + tid < nfluid) acc[c] += (double)su[c][tid];
+        if (tile_start + tid + TPB < nfluid) acc[c] += (double)su[c][tid + TPB];
+    }
+}
+
 // Odd (local) step with two adjacent pore voxels (i, i + 1), i even, per
 // thread: every slot pair of a plane is one aligned 8-byte (FP32) or 4-byte
 // (16-bit) access, the two voxels collide together in packed FP32, and the
 // 16-bit types round both values with one cvt.rs fed with the bits each would
-// get alone, so the populations equal those of step3d_odd_kernel (the flux
-// partials are summed in another order).  The
+// get alone, so the populations equal those of step3d_odd_kernel, and the
+// flux partials are summed in its order (canonical_acc).  The
 // partner of the last voxel of an odd-sized lattice is a padding slot (the
 // plane stride is a multiple of 64); it is read and written but never used.
 template <class ST, int MINB, bool W1>
@@ -605,6 +629,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepAr
     using T = typename ST::T;
     static_assert(TILE_NPT == 2, "a tile is one voxel pair per thread");
     __shared__ double sh[TPB / 32][3];
+    __shared__ float su[3][TPB * TILE_NPT];
     const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const int2 item = a.work[w];
@@ -616,10 +641,11 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepAr
         T *__restrict__ A = static_cast<T *>(S.A);
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
-        const unsigned i0 = (unsigned)(item.y * (TPB * TILE_NPT) + 2 * threadIdx.x);
+        const unsigned ts = (unsigned)item.y * (TPB * TILE_NPT);
+        const unsigned i0 = ts + 2u * threadIdx.x;
+        float2 u[3] = {};
         if (i0 < (unsigned)S.nfluid) {
-            const bool v1 = i0 + 1u < (unsigned)S.nfluid;
-            float2 g[Q3], u[3];
+            float2 g[Q3];
 #pragma unroll
             for (int k = 0; k < Q3; ++k) ST::ld2(A + (k * P + i0), g[k].x, g[k].y);
             collide3x2<ST, W1>(g, S, u);
@@ -627,10 +653,11 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepAr
 #pragma unroll
             for (int k = 0; k < Q3; ++k)
                 ST::st2(A + (opp3(k) * P + i0), g[k].x, g[k].y, dir_bits(h0, k), dir_bits(h1, k));
-            acc[0] += (double)u[0].x; acc[1] += (double)u[1].x; acc[2] += (double)u[2].x;
-            if (v1) { acc[0] += (double)u[0].y; acc[1] += (double)u[1].y; acc[2] += (double)u[2].y; }
         }
-        if (red) finish_tile(S, item.y, n, acc, sh);
+        if (red) {
+            canonical_acc<TPB, 0>(su, u, threadIdx.x, ts, (unsigned)S.nfluid, acc);
+            finish_tile(S, item.y, n, acc, sh);
+        }
     }
 }
 
@@ -670,6 +697,7 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
     __shared__ uint64_t full[NS], empty[NS];
     __shared__ int slot_item[NS];
     __shared__ double sh[TPB / 32][3];
+    __shared__ float su[3][TPB * TILE_NPT];
     const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
     const int tid = threadIdx.x;
     const unsigned long long wait_ns = a.wait_ns ? a.wait_ns : WAIT_NS;
@@ -779,22 +807,23 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
         const unsigned P = (unsigned)S.plane;
         const T *buf = reinterpret_cast<const T *>(ring + s * (Q3 * RUN));
         double acc[3] = {0.0, 0.0, 0.0};
-        const unsigned i0 = (unsigned)item.y * TV + 2u * tid;
-        float2 g[Q3], u[3];
+        const unsigned ts = (unsigned)item.y * TV;
+        const unsigned i0 = ts + 2u * tid;
+        float2 g[Q3], u[3] = {};
 #pragma unroll
         for (int k = 0; k < Q3; ++k) ST::lds2(buf + (k * TV + 2u * tid), g[k].x, g[k].y);
         mbar_arrive(&empty[s]);    // this thread is done with buffer s
         if (i0 < (unsigned)S.nfluid) {
-            const bool v1 = i0 + 1u < (unsigned)S.nfluid;
             collide3x2<ST, W1>(g, S, u);
             const uint32_t h0 = voxel_bits<ST>(i0, n), h1 = voxel_bits<ST>(i0 + 1u, n);
 #pragma unroll
             for (int k = 0; k < Q3; ++k)
                 ST::st2(A + (opp3(k) * P + i0), g[k].x, g[k].y, dir_bits(h0, k), dir_bits(h1, k));
-            acc[0] += (double)u[0].x; acc[1] += (double)u[1].x; acc[2] += (double)u[2].x;
-            if (v1) { acc[0] += (double)u[0].y; acc[1] += (double)u[1].y; acc[2] += (double)u[2].y; }
         }
-        if (red) finish_tile<TPB, BAR>(S, item.y, n, acc, sh);
+        if (red) {
+            canonical_acc<TPB, BAR>(su, u, tid, ts, (unsigned)S.nfluid, acc);
+            finish_tile<TPB, BAR>(S, item.y, n, acc, sh);
+        }
     }
 }
 

@@ -184,8 +184,8 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     b->precision = precision;
     b->chunk = chunk;
     b->budget = hbm_budget;
-    b->variant = 0;
-    b->npt = variant_npt(precision, 0);
+    b->variant = lbm_default_variant(precision);
+    b->npt = variant_npt(precision, b->variant);
     b->cap_slots = 4096;
     b->cap_work = 1 << 16;
     b->slots.resize(b->cap_slots);

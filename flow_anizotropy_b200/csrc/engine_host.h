@@ -21,6 +21,8 @@ struct lbm_ctx {
 
 int lbm_fail_cuda(lbm_ctx *ctx, cudaError_t e, const char *what, int line);
 int lbm_fail_input(lbm_ctx *ctx, const std::string &msg);
+// The step-kernel variant LBM_VARIANT_DEFAULT stands for.
+int lbm_default_variant(int prec);
 bool lbm_is_device_ptr(const void *p);
 std::string &lbm_last_error_global();
 

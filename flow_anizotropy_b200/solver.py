@@ -38,7 +38,7 @@ class Params3D:
     criterion: str = "auto"     # "drift" (reference), "block", or auto: block for fp16/bf16
     sample: int = 10
     ksigma: float = 3.0
-    variant: int = 0
+    variant: int = _lib.LBM_VARIANT_DEFAULT   # or an index from tune3d
 
     def to_c(self) -> _lib.Params3D:
         prec = _lib.PRECISIONS[self.precision]

@@ -41,6 +41,11 @@ extern "C" {
 #define LBM_EBUSY          4
 #define LBM_ECUDA        (-1)
 
+/* lbm_params3d.variant: the library's default for the precision (the
+ * variant the autotuner picks on the 128^3 tensor workload: FP32 3, FP16 and
+ * BF16 33, 0 otherwise).  Every variant of a precision gives the same bits. */
+#define LBM_VARIANT_DEFAULT (-1)
+
 /* Population storage (collision arithmetic is FP64 for LBM_FP64, else FP32;
  * flux reductions, convergence test and averaging are FP64 in every mode). */
 #define LBM_FP64  0   /* f_k as double, the reference's own arithmetic           */
@@ -76,7 +81,7 @@ typedef struct {
     int       hold;
     int       precision;
     int       criterion;
-    int       variant;      /* step-kernel variant (see lbm_tune3d); 0 = default */
+    int       variant;      /* step-kernel variant (see lbm_tune3d), or LBM_VARIANT_DEFAULT */
     long long sample;       /* LBM_CRIT_BLOCK sample interval                 */
     double    ksigma;       /* LBM_CRIT_BLOCK acceptance                      */
 } lbm_params3d;

@@ -98,3 +98,20 @@ def test_starved_waits_end_with_status(gpu):
     ok, rc, _ = S.solve3d(solid, [[F, 0, 0]], p)
     ref, rc0, _ = S.solve3d(solid, [[F, 0, 0]], S.Params3D(precision="fp16", variant=_variant(PAIR), **prm))
     assert rc == rc0 and ok[0].steps == ref[0].steps and np.array_equal(ok[0].q, ref[0].q)
+
+
+@pytest.mark.parametrize("prec,default", [("fp32", 3), ("fp16", 33), ("bf16", 33), ("fp64", 0)])
+def test_default_variant_is_the_tuned_pick_and_matches_variant_0(gpu, prec, default):
+    """LBM_VARIANT_DEFAULT runs the listed variant; since every variant sums
+    the fluxes in one order, a whole solve with it equals variant 0's bits."""
+    solid = st.sphere_packing((20, 24, 28), 4.0, 0.6, seed=11, percolate=(True, True, True))
+    F = 1e-6
+    forces = [[F, 0, 0], [0, 0, F]]
+    prm = dict(eps=1e-7, lag=200, hold=2, min_steps=400, max_steps=4000, avg_steps=100, precision=prec)
+    runs = {}
+    for v in (-1, default, 0):
+        runs[v] = S.solve3d(solid, forces, S.Params3D(variant=v, **prm))[0]
+    for v in (default, 0):
+        for a, b in zip(runs[-1], runs[v]):
+            assert (a.steps, a.converged) == (b.steps, b.converged)
+            assert np.array_equal(a.q, b.q) and np.array_equal(a.se, b.se), (prec, v)
