@@ -268,13 +268,15 @@ def serve_trace(device, prec, args):
     wall = time.perf_counter() - t0
     srv.close()
     served = stats.completed / wall
-    # plain FP32 on the same structures, one tensor at a time (one launch per
-    # step): the baseline the served throughput is compared with
-    pp = Params3D(**{**p.__dict__, "precision": "fp32"})
+    # plain FP32 on the same structures, one tensor at a time, each with the
+    # step-kernel variant the autotuner picks for it (tuning not timed): the
+    # baseline the served throughput is compared with
     from flow_anizotropy_b200 import solver as S
-    S.solve3d(pool[0], forces, pp, device=device)
+    tuned = [S.tune3d(s_, ndir=3, precision="fp32", nsteps=100, device=device)[0] for s_ in pool]
+    pps = [Params3D(**{**p.__dict__, "precision": "fp32", "variant": v}) for v in tuned]
+    S.solve3d(pool[0], forces, pps[0], device=device)
     t0 = time.perf_counter()
-    for s_ in pool:
+    for s_, pp in zip(pool, pps):
         S.solve3d(s_, forces, pp, device=device)
     plain = len(pool) / (time.perf_counter() - t0)
     return {"rate_per_s": 20.0, "arrival_seconds": args.serve_seconds, "requests": stats.completed,
@@ -377,7 +379,9 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg_bytes / (head["ms"] / 1e3) / 1e9
     per_launch_alg = alg_bytes / max(1, head["launches"])
     traffic = profiled_traffic(head_prec)
-    serving = serve_trace(device, head_prec, args) if args.serve_seconds > 0 else None
+    # served in FP32: on the small serving structures FP16 needs up to 6x the
+    # steps under its criterion (measured 42000 against 7000), so FP32 serves more
+    serving = serve_trace(device, args.serve_precision, args) if args.serve_seconds > 0 else None
     out = None
     if rank == 0:
         cpu = cpu_sample(solid, wl, seconds_target=args.cpu_seconds)
@@ -588,6 +592,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32", "md32"])
     ap.add_argument("--serve-seconds", type=float, default=5.0)
+    ap.add_argument("--serve-precision", default="fp32", choices=["fp32", "fp16", "bf16"])
     ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch", "gen3d", "large"])
     ap.add_argument("--large-n", type=int, default=512, help="cell edge of the large workload")
     ap.add_argument("--large-steps", type=int, default=2000)

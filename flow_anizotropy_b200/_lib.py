@@ -24,7 +24,7 @@ CRIT_DRIFT, CRIT_BLOCK = 0, 1
 SYMBOLS = (
     "lbm_version", "lbm_create", "lbm_destroy", "lbm_last_error", "lbm_stream",
     "lbm_solve3d", "lbm_solve2d", "lbm_solve2d_many", "lbm_solve2d_noalloc",
-    "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_bytes3d", "lbm_batch_submit3d",
+    "lbm_batch_create", "lbm_batch_set_variant", "lbm_batch_destroy", "lbm_batch_bytes3d", "lbm_batch_submit3d",
     "lbm_batch_run", "lbm_batch_poll", "lbm_batch_active", "lbm_batch_resident_bytes",
     "lbm_variant_count", "lbm_tune3d",
     "lbm_debug_steps3d", "lbm_debug_steps2d", "lbm_debug_bulk_wait",
@@ -105,6 +105,8 @@ def load(path: Path | str | None = None):
         L.lbm_solve2d_noalloc.restype = C.c_int
         L.lbm_batch_create.argtypes = [vp, C.POINTER(vp), C.c_int, C.c_longlong, C.c_int]
         L.lbm_batch_create.restype = C.c_int
+        L.lbm_batch_set_variant.argtypes = [vp, C.c_int]
+        L.lbm_batch_set_variant.restype = C.c_int
         L.lbm_batch_destroy.argtypes = [vp]
         L.lbm_batch_destroy.restype = None
         L.lbm_batch_bytes3d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]

@@ -208,6 +208,21 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     return LBM_OK;
 }
 
+extern "C" int lbm_batch_set_variant(lbm_batch *b, int variant)
+{
+    if (!b) return LBM_EINPUT;
+    lbm_ctx *ctx = b->ctx;
+    if (variant == LBM_VARIANT_DEFAULT) variant = lbm_default_variant(b->precision);
+    if (variant < 0 || variant >= variant_count(b->precision))
+        return lbm_fail_input(ctx, "unknown step-kernel variant");
+    for (const Slot &s : b->slots)
+        if (s.used) return lbm_fail_input(ctx, "the batch has resident solves");
+    if (variant_npt(b->precision, variant) != b->npt) return lbm_fail_input(ctx, "variant changes the tile size");
+    b->variant = variant;
+    b->graph_nwork = -1;      // recapture with the new kernels at the next change
+    return LBM_OK;
+}
+
 extern "C" void lbm_batch_destroy(lbm_batch *b)
 {
     if (!b) return;

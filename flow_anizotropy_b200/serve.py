@@ -59,11 +59,12 @@ class Server:
     """Continuous-batching solver for one precision and one device."""
 
     def __init__(self, precision="fp32", hbm_budget=150 * 2**30, chunk=256, device=0, clock=time.perf_counter,
-                 max_work=2_000_000, batch=None):
+                 max_work=2_000_000, batch=None, variant=-1):
         # `batch` replaces the device batch (an object with the Batch methods
-        # submit/run/poll/resident_bytes/close), for testing the scheduling
+        # submit/run/poll/resident_bytes/close), for testing the scheduling;
+        # `variant` is the step-kernel variant of the batch (-1: the default)
         self.batch = batch if batch is not None else Batch(precision=precision, hbm_budget=hbm_budget,
-                                                           chunk=chunk, device=device)
+                                                           chunk=chunk, device=device, variant=variant)
         self.max_work = max_work
         self.resident_work = 0
         self.precision = precision

@@ -248,7 +248,8 @@ class Batch:
     returns the structures whose every direction has finished.
     """
 
-    def __init__(self, precision="fp16", hbm_budget=150 * 2**30, chunk=64, device=0):
+    def __init__(self, precision="fp16", hbm_budget=150 * 2**30, chunk=64, device=0,
+                 variant=_lib.LBM_VARIANT_DEFAULT):
         self.ctx = _lib.context(device)
         self.precision = precision
         h = C.c_void_p()
@@ -256,6 +257,8 @@ class Batch:
                                                    _lib.PRECISIONS[precision],
                                                    int(hbm_budget), int(chunk)))
         self.h = h
+        if variant != _lib.LBM_VARIANT_DEFAULT:
+            self.ctx.check(self.ctx.L.lbm_batch_set_variant(h, int(variant)))
         self.chunk = chunk
         self._pending: dict[int, _Pending] = {}
 

@@ -191,6 +191,12 @@ typedef struct lbm_batch lbm_batch;
  * the device memory the batch may hold for lattices, in bytes. */
 int  lbm_batch_create(lbm_ctx *ctx, lbm_batch **batch, int precision,
                       long long hbm_budget, int chunk);
+
+/* Step-kernel variant of every launch of an empty batch (default
+ * LBM_VARIANT_DEFAULT, the variant lbm_tune3d picks on the 128^3 tensor
+ * workload; mixes of small structures may prefer another).  Results do not
+ * depend on it.  LBM_EINPUT while solves are resident. */
+int  lbm_batch_set_variant(lbm_batch *batch, int variant);
 void lbm_batch_destroy(lbm_batch *batch);
 
 /* Upper bound on the device bytes one structure with ndir directions

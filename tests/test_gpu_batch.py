@@ -94,3 +94,35 @@ def test_batch_mixed_tau(gpu):
         for a, m in zip(alone, done[tag]):
             assert a.steps == m.steps
             np.testing.assert_allclose(m.q, a.q, rtol=1e-6, atol=1e-20)
+
+
+def test_batch_variant_choice(gpu):
+    """lbm_batch_set_variant: any variant gives the default's bits; it is
+    refused while solves are resident and for an unknown index."""
+    from flow_anizotropy_b200 import _lib
+    structs = _mix()[:2]
+    p = S.Params3D(precision="fp16", **PRM)
+    out = {}
+    for v in (-1, 1, 25):
+        b = S.Batch(precision="fp16", hbm_budget=4 * 2**30, chunk=32, variant=v)
+        for t, s in enumerate(structs):
+            assert b.submit(s, _forces(), p, tag=t)
+        with pytest.raises(_lib.LBMError):
+            b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, 0))
+        done = {}
+        for _ in range(1000):
+            b.run(4)
+            for tag, runs in b.poll():
+                done[tag] = runs
+            if len(done) == len(structs):
+                break
+        out[v] = done
+        b.close()
+    for v in (1, 25):
+        for t in range(len(structs)):
+            for a, m in zip(out[-1][t], out[v][t]):
+                assert a.steps == m.steps and np.array_equal(a.q, m.q) and np.array_equal(a.se, m.se), v
+    b = S.Batch(precision="fp16", hbm_budget=4 * 2**30, chunk=32)
+    with pytest.raises(_lib.LBMError):
+        b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, 10**6))
+    b.close()
