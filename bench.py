@@ -556,6 +556,72 @@ def run_gen_workload(args, device=0):
             "speedup_vs_cpu_core": (n / wall) / (cpu_n / cpu), "identical_structures": same}
 
 
+def run_perm2d_workload(args, device=0):
+    """D2Q9 permeability (the 2D drop-in's solve) of --count seeded 256^2
+    disc packings (solid fraction 0.2-0.4), forcing along x and y, the 2D
+    reference's default convergence knobs, --group2d images per launch
+    (lbm_solve2d_many): images/s, fluid GLUPS and the HBM roofline (72 B per
+    fluid-cell update) against the reference binary lbm2d-perm on all host
+    cores (fixed-step sample per process, extrapolated with the device step
+    counts, which equal the reference's: the 2D path is bit-identical)."""
+    import torch
+    from oracle import oracle as O
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200 import solver as S
+    from flow_anizotropy_b200 import structures as st
+    from flow_anizotropy_b200.structure_io import save_dat
+    n, group = args.count, args.group2d
+    imgs = np.stack([st.disc_packing_2d(seed=i, solid_fraction=0.2 + 0.05 * (i % 5)) for i in range(n)])
+    F = S.FX_BASE
+    forces = [[F, 0.0], [0.0, F]]
+    p = S.Params2D()
+    ctx = _lib.context(device)
+    S.solve2d_many(imgs[:min(group, n)], forces, S.Params2D(max_steps=200, min_steps=100, lag=100, avg_steps=0),
+                   device=device)
+    runs = []
+    with Clocks(device) as clk, EventTimer(torch, ctx.stream) as t:
+        t0 = time.perf_counter()
+        for g in range(0, n, group):
+            runs += S.solve2d_many(imgs[g:g + group], forces, p, device=device)[0]
+        wall = time.perf_counter() - t0
+    steps = [r.steps for rr in runs for r in rr]
+    fluid = float((imgs == 0).sum(axis=(1, 2)).mean())
+    upd = sum(r.steps * float((img == 0).sum()) for img, rr in zip(imgs, runs) for r in rr)
+    peak, peak_kind = measured_peak()
+    ab = 72.0 * upd
+    out = {"workload": f"D2Q9 256^2 disc packings, {n} images x 2 directions, reference 2D defaults "
+                       f"(eps 1e-3, lag 5000, min 10000, avg 20000), {group} images per launch",
+           "images_per_s": n / (t.ms / 1e3), "images_per_s_wall": n / wall, "device_ms": t.ms,
+           "glups_fluid": upd / (t.ms / 1e3) / 1e9, "mean_fluid_cells": fluid,
+           "steps_min_max": [min(steps), max(steps)], "converged": sum(r.converged for rr in runs for r in rr),
+           "roofline": {"bound": "hbm", "achieved": ab / (t.ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": ab / (t.ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+           "clocks": clk.summary()}
+    ref = O.ref_binary("lbm2d-perm")
+    if ref is not None:
+        cores = os.cpu_count() or 1
+        sample_steps = max(2, int(args.cpu_seconds * 20e6 / (2 * 65536)))   # ~20 MLUPS per core
+        tmp = Path(tempfile.mkdtemp(prefix="lbm2dcpu_"))
+        save_dat(tmp / "s.dat", imgs[0])
+        argv = ["--quiet", "--max-steps", str(sample_steps), "--min-steps", str(sample_steps + 1),
+                "--lag", str(sample_steps + 1), "--avg-steps", "0", "--avg-sample", "1"]
+        t0 = time.perf_counter()
+        procs = [subprocess.Popen([str(ref), str(tmp / "s.dat"), str(tmp / f"o{i}.csv")] + argv,
+                                  stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for i in range(cores)]
+        for pr in procs:
+            pr.wait()
+        dt = time.perf_counter() - t0
+        shutil.rmtree(tmp, ignore_errors=True)
+        lups = 2 * sample_steps * 65536 / dt          # per process, all cells
+        sec_image = sum(steps) / n * 65536 / lups     # both directions of a mean image
+        out["cpu_baseline"] = {"images_per_s": cores / sec_image, "cores": cores, "kind": "reference",
+                               "mlups_per_core": lups / 1e6,
+                               "sample": f"2 x {sample_steps} fixed steps of a 256^2 image per process, "
+                                         f"{cores} processes; extrapolated with the device step counts"}
+        out["speedup_vs_cpu"] = out["images_per_s"] / out["cpu_baseline"]["images_per_s"]
+    return out
+
+
 # -------------------------------------------------------- reference arm ----
 def run_reference(args, rank, world):
     if rank != 0:
@@ -593,7 +659,8 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32", "md32"])
     ap.add_argument("--serve-seconds", type=float, default=5.0)
     ap.add_argument("--serve-precision", default="fp32", choices=["fp32", "fp16", "bf16"])
-    ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch", "gen3d", "large"])
+    ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch", "gen3d", "large", "perm2d"])
+    ap.add_argument("--group2d", type=int, default=16, help="images per launch of the perm2d workload")
     ap.add_argument("--large-n", type=int, default=512, help="cell edge of the large workload")
     ap.add_argument("--large-steps", type=int, default=2000)
     ap.add_argument("--gen-size", type=int, default=80, help="cell edge of the gen3d workload")
@@ -612,6 +679,8 @@ def main():
         out = run_gen_workload(args, local_rank) if rank == 0 else None
     elif args.workload == "large":
         out = run_large_workload(args, local_rank) if rank == 0 else None
+    elif args.workload == "perm2d":
+        out = run_perm2d_workload(args, local_rank) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None and rank == 0:

@@ -140,13 +140,18 @@ static int setup2d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int ndir,
     if (rc) return rc;
     set.hs.resize(ndir);
     set.hst.resize(ndir);
-    set.bufs.reserve(4 * ndir);
+    set.bufs.reserve(4 * ndir + 1);
+    set.bufs.emplace_back(ctx->stream);                 // neighbour solid bits, shared by the directions
+    DevMem &nbm = set.bufs.back();
+    CK(nbm.alloc(sizeof(uint16_t) * (size_t)nx * ny));
+    CK(launch_nbmask2d(static_cast<const uint32_t *>(mask.p), nx, ny, static_cast<uint16_t *>(nbm.p), ctx->stream));
+    const uint16_t *nbm_p = static_cast<const uint16_t *>(nbm.p);
     CK(d_states.alloc(sizeof(State2) * ndir));
     for (int j = 0; j < ndir; ++j) {
         Solve2 &S = set.hs[j];
         fill_solve2(S, nx, ny, forces + 2 * j, p);
         for (int b = 0; b < 4; ++b) set.bufs.emplace_back(ctx->stream);
-        DevMem *B = &set.bufs[4 * j];
+        DevMem *B = &set.bufs[1 + 4 * j];
         CK(B[0].alloc(sizeof(float) * Q2 * (size_t)S.plane));
         CK(B[1].alloc(sizeof(double) * 2 * (size_t)S.ntiles));
         CK(B[2].alloc(sizeof(float) * 2 * (size_t)S.nn));
@@ -158,6 +163,7 @@ static int setup2d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, int ndir,
         S.snap = static_cast<float *>(B[2].p);
         S.last = static_cast<float *>(B[3].p);
         S.mask = static_cast<const uint32_t *>(mask.p);
+        S.nbm = nbm_p;
         S.st = static_cast<State2 *>(d_states.p) + j;
         init_state2(set.hst[j], S.c);
         init2d_kernel<<<256, 256, 0, ctx->stream>>>(S.A, S.plane, S.nn);
@@ -253,8 +259,9 @@ extern "C" int lbm_solve2d_many(lbm_ctx *ctx, int nstruct, const uint8_t *solids
     int rc = check_params2d(ctx, p);
     if (rc) return rc;
     const int nsolve = nstruct * ndir;
-    std::vector<DevMem> masks;
+    std::vector<DevMem> masks, nbms;
     masks.reserve(nstruct);
+    nbms.reserve(nstruct);
     std::vector<Solve2> hs(nsolve);
     std::vector<State2> hst(nsolve);
     std::vector<DevMem> bufs;
@@ -269,6 +276,10 @@ extern "C" int lbm_solve2d_many(lbm_ctx *ctx, int nstruct, const uint8_t *solids
             ctx->err = "structure " + std::to_string(k) + ": " + ctx->err;
             return rc;
         }
+        nbms.emplace_back(ctx->stream);
+        CK(nbms.back().alloc(sizeof(uint16_t) * (size_t)nn));
+        CK(launch_nbmask2d(static_cast<const uint32_t *>(masks.back().p), nx, ny,
+                           static_cast<uint16_t *>(nbms.back().p), ctx->stream));
         for (int j = 0; j < ndir; ++j) {
             const int id = k * ndir + j;
             Solve2 &S = hs[id];
@@ -286,6 +297,7 @@ extern "C" int lbm_solve2d_many(lbm_ctx *ctx, int nstruct, const uint8_t *solids
             S.snap = static_cast<float *>(B[2].p);
             S.last = static_cast<float *>(B[3].p);
             S.mask = static_cast<const uint32_t *>(masks.back().p);
+            S.nbm = static_cast<const uint16_t *>(nbms.back().p);
             S.st = static_cast<State2 *>(d_states.p) + id;
             init_state2(hst[id], S.c);
             init2d_kernel<<<256, 256, 0, ctx->stream>>>(S.A, S.plane, S.nn);

@@ -59,7 +59,7 @@ constexpr size_t al256(size_t n) { return (n + 255) / 256 * 256; }
 // Byte layout of the scratch array.  Per direction: the AA lattice (9 planes),
 // the U,V snapshot and last fields, the per-tile flux partials.  Shared: the
 // bit mask (ceil(nx/32) * ny <= nx * ny words), the byte mask staged from
-// host memory, controller states, solve records, the work list, and the
+// host memory, the neighbour solid bits (one 16-bit word per cell), controller states, solve records, the work list, and the
 // small sums (fieldres numerator/denominator per direction, pore count and
 // the non-binary flag of the mask packing).
 constexpr size_t kLatBytes = al256(sizeof(float) * Q2 * kCells);
@@ -68,7 +68,8 @@ constexpr size_t kPartBytes = al256(sizeof(double) * 2 * kTiles);
 constexpr size_t kDirBytes = kLatBytes + 2 * kFieldBytes + kPartBytes;
 constexpr size_t kMaskOff = kDirs * kDirBytes;
 constexpr size_t kSolidOff = kMaskOff + al256(sizeof(uint32_t) * kCells);
-constexpr size_t kStateOff = kSolidOff + al256((size_t)kCells);
+constexpr size_t kNbmOff = kSolidOff + al256((size_t)kCells);
+constexpr size_t kStateOff = kNbmOff + al256(sizeof(uint16_t) * kCells);
 constexpr size_t kSolveOff = kStateOff + al256(sizeof(State2) * kDirs);
 constexpr size_t kWorkOff = kSolveOff + al256(sizeof(Solve2) * kDirs);
 constexpr size_t kSmallOff = kWorkOff + al256(sizeof(int2) * kDirs * kTiles);
@@ -147,6 +148,8 @@ extern "C" int lbm_solve2d_noalloc(lbm_ctx *ctx, const uint8_t *solid, int nx, i
     CK(cudaStreamSynchronize(st));
     if ((unsigned)h[1]) return lbm_fail_input(ctx, "non-binary voxel");
     if (h[0] == 0) return lbm_fail_input(ctx, "structure has no pore space");
+    auto *nbm = reinterpret_cast<uint16_t *>(base + kNbmOff);
+    CK(launch_nbmask2d(mask, nx, ny, nbm, st));
 
     // per-direction solve records on the scratch
     auto *d_states = reinterpret_cast<State2 *>(base + kStateOff);
@@ -165,6 +168,7 @@ extern "C" int lbm_solve2d_noalloc(lbm_ctx *ctx, const uint8_t *solid, int nx, i
         S.last = reinterpret_cast<float *>(d + kLatBytes + kFieldBytes);
         S.partials = reinterpret_cast<double *>(d + kLatBytes + 2 * kFieldBytes);
         S.mask = mask;
+        S.nbm = nbm;
         S.st = d_states + j;
         // the fields are read back for cells a step never writes (solids), so
         // they start at zero as in lbm_solve2d; lattice and partials are

@@ -48,6 +48,7 @@ struct Solve2 {
     float *A;
     unsigned plane;
     const uint32_t *mask;
+    const uint16_t *nbm;   // per cell: bit k set if the cell at offset e_k is solid (k = 0: itself)
     int nx, ny, wpr;
     int nn;
     int ntiles;
@@ -238,12 +239,15 @@ __device__ __forceinline__ void collide2(float (&g)[Q2], float fx, float fy, flo
     }
 }
 
-__global__ void __launch_bounds__(TPB) step2d_kernel(const StepArgs2 a);
+__global__ void __launch_bounds__(TPB, 4) step2d_kernel(const StepArgs2 a);
 __global__ void init2d_kernel(float *A, unsigned plane, int nn);
+// Neighbour solid bits of every cell (Solve2::nbm) from the bit mask.
+__global__ void nbmask2d_kernel(const uint32_t *mask, int nx, int ny, int wpr, uint16_t *nbm);
 __global__ void canon2d_kernel(const Solve2 S, long long done, float *f_out);
 __global__ void fieldres2d_kernel(const float *snap, const float *last, int nn, double *out);
 
 cudaError_t launch_step2d(dim3 grid, cudaStream_t s, const StepArgs2 &a);
 cudaError_t launch_advance2d(const Solve2 *solves, int nsolves, long long steps, cudaStream_t s);
+cudaError_t launch_nbmask2d(const uint32_t *mask, int nx, int ny, uint16_t *nbm, cudaStream_t s);
 
 }  // namespace lbm

@@ -5,7 +5,7 @@
 
 namespace lbm {
 
-__global__ void __launch_bounds__(TPB) step2d_kernel(const StepArgs2 a)
+__global__ void __launch_bounds__(TPB, 4) step2d_kernel(const StepArgs2 a)
 {
     __shared__ double sh[TPB / 32][3];
     for (int w = blockIdx.x; w < a.nwork; w += gridDim.x) {
@@ -30,14 +30,10 @@ __global__ void __launch_bounds__(TPB) step2d_kernel(const StepArgs2 a)
             const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
             const int X[3] = {xm, x, xp};
             const int Yr[3] = {ym, y, yp};
-            uint32_t sol = 0;
+            const uint32_t sol = S.nbm[nd];
             int idx[Q2];
 #pragma unroll
-            for (int k = 0; k < Q2; ++k) {
-                const int yy = Yr[ey2(k) + 1], xx = X[ex2(k) + 1];
-                idx[k] = yy * nx + xx;
-                sol |= (uint32_t)mbit(S.mask + (size_t)yy * S.wpr, xx) << k;
-            }
+            for (int k = 0; k < Q2; ++k) idx[k] = Yr[ey2(k) + 1] * nx + X[ex2(k) + 1];
             float U = 0.0f, V = 0.0f;
             if (!(sol & 1u)) {
                 float g[Q2];
@@ -71,6 +67,30 @@ __global__ void __launch_bounds__(TPB) step2d_kernel(const StepArgs2 a)
         }
         if (red) finish_tile2(S, item.y, n, acc, sh);
     }
+}
+
+__global__ void nbmask2d_kernel(const uint32_t *mask, int nx, int ny, int wpr, uint16_t *nbm)
+{
+    const int nn = nx * ny;
+    for (int nd = blockIdx.x * blockDim.x + threadIdx.x; nd < nn; nd += gridDim.x * blockDim.x) {
+        const int y = nd / nx, x = nd - y * nx;
+        const int X[3] = {x == 0 ? nx - 1 : x - 1, x, x == nx - 1 ? 0 : x + 1};
+        const int Yr[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
+        uint32_t sol = 0;
+#pragma unroll
+        for (int k = 0; k < Q2; ++k) {
+            const int yy = Yr[ey2(k) + 1], xx = X[ex2(k) + 1];
+            sol |= (uint32_t)mbit(mask + (size_t)yy * wpr, xx) << k;
+        }
+        nbm[nd] = (uint16_t)sol;
+    }
+}
+
+cudaError_t launch_nbmask2d(const uint32_t *mask, int nx, int ny, uint16_t *nbm, cudaStream_t s)
+{
+    const int nn = nx * ny;
+    nbmask2d_kernel<<<(nn + 255) / 256 < 1184 ? (nn + 255) / 256 : 1184, 256, 0, s>>>(mask, nx, ny, (nx + 31) / 32, nbm);
+    return cudaGetLastError();
 }
 
 __global__ void init2d_kernel(float *A, unsigned plane, int nn)

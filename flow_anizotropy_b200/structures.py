@@ -266,6 +266,21 @@ def batch_mix(count=256, seed=0, sizes=(48, 64, 96, 128, 160)):
     return out
 
 
+def disc_packing_2d(seed, solid_fraction, n=256, rmin=4, rmax=12):
+    """Periodic 2D cell (the D2Q9 reference's fixed 256 x 256) of overlapping
+    discs, radius U{rmin..rmax-1}, added until the solid fraction reaches
+    ``solid_fraction``; [y, x] uint8, 1 = solid."""
+    rng = np.random.default_rng(seed)
+    s = np.zeros((n, n), np.uint8)
+    yy, xx = np.mgrid[0:n, 0:n]
+    while s.mean() < solid_fraction:
+        cx, cy, r = rng.integers(0, n), rng.integers(0, n), rng.integers(rmin, rmax)
+        dx = np.minimum(np.abs(xx - cx), n - np.abs(xx - cx))
+        dy = np.minimum(np.abs(yy - cy), n - np.abs(yy - cy))
+        s[dx * dx + dy * dy <= r * r] = 1
+    return s
+
+
 def make(d):
     """Build one structure from a batch_mix / serving description."""
     if d["kind"] == "grf":
