@@ -96,7 +96,7 @@ class Clocks:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,clocks.mem")
 
     def __init__(self, device):
         self.device = device
@@ -122,7 +122,7 @@ class Clocks:
         if not self.p:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.f.seek(0)
-        sm, smax, reasons = [], [], set()
+        sm, smax, mem, watts, reasons = [], [], [], [], set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
         for line in self.f:
             parts = [x.strip() for x in line.split(",")]
@@ -131,6 +131,9 @@ class Clocks:
             try:
                 sm.append(float(parts[1]))
                 smax.append(float(parts[2]))
+                watts.append(float(parts[3]))
+                if len(parts) > 9:
+                    mem.append(float(parts[9]))
             except ValueError:
                 continue
             for nm, v in zip(names, parts[5:9]):
@@ -138,6 +141,8 @@ class Clocks:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
+                "mem_mhz": statistics.median(mem) if mem else None,
+                "power_w": statistics.median(watts) if watts else None,
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
@@ -393,7 +398,8 @@ def run_ours(args, rank, world, local_rank):
                          "steps_per_direction": [r.steps for r in m["runs"]],
                          "converged": [r.converged for r in m["runs"]],
                          "rel_err_vs_fp64": m["err"], "kernel_variant": m["variant"],
-                         "hbm_gbs_alg": m["dir_steps"] * alg_bytes_per_dir_step(p_, npore, N) / (m["ms"] / 1e3) / 1e9}
+                         "hbm_gbs_alg": m["dir_steps"] * alg_bytes_per_dir_step(p_, npore, N) / (m["ms"] / 1e3) / 1e9,
+                         "clocks": m["clocks"]}
         out = {
             "metric": METRIC, "value": kt, "unit": "k-tensors/hr", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
