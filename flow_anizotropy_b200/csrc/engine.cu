@@ -114,6 +114,15 @@ extern "C" int lbm_create(lbm_ctx **out, int device)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = prepare_step3d_lp(device);
+    if (e == cudaSuccess) {
+        // keep up to 4 GiB of freed lattices in the device's stream-ordered
+        // pool between solves instead of returning them to the driver at
+        // every synchronisation (repeated solves then reuse mapped memory)
+        cudaMemPool_t pool = nullptr;
+        e = cudaDeviceGetDefaultMemPool(&pool, device);
+        unsigned long long keep = 4ull << 30;
+        if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (e != cudaSuccess) {
         lbm_last_error_global() = std::string("CUDA error: ") + cudaGetErrorString(e);
         delete ctx;
