@@ -327,7 +327,7 @@ struct StoreF16 {
     }
     __device__ static __forceinline__ void st2(T *p, C lo, C hi, uint32_t rlo, uint32_t rhi)
     {
-        const uint32_t rb = (__funnelshift_l(rhi, rhi, 16) << 16) | (__funnelshift_l(rlo, rlo, 16) & 0xffffu);
+        const uint32_t rb = __byte_perm(rlo, rhi, 0x7632);   // high halves: rhi above, rlo below
         uint32_t d;
         asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rb));
         __stcs(reinterpret_cast<unsigned int *>(p), d);
@@ -370,7 +370,7 @@ struct StoreBF16 {
     }
     __device__ static __forceinline__ void st2(T *p, C lo, C hi, uint32_t rlo, uint32_t rhi)
     {
-        const uint32_t rb = (__funnelshift_l(rhi, rhi, 16) << 16) | (__funnelshift_l(rlo, rlo, 16) & 0xffffu);
+        const uint32_t rb = __byte_perm(rlo, rhi, 0x7632);   // high halves: rhi above, rlo below
         uint32_t d;
         asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rb));
         __stcs(reinterpret_cast<unsigned int *>(p), d);
