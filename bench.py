@@ -409,7 +409,7 @@ def run_ours(args, rank, world, local_rank):
                        "eps": wl["eps"], "lag": wl["lag"], "hold": wl["hold"], "min_steps": wl["min_steps"],
                        "max_steps": wl["max_steps"], "avg_steps": wl["avg_steps"],
                        "path": head_prec, "kernel_variant": head["variant"],
-                       "criterion": "block-mean k-sigma" if head_prec in ("fp16", "bf16") else "drift (reference)",
+                       "criterion": "block means, batch-means SE, k-sigma" if head_prec in ("fp16", "bf16") else "drift (reference)",
                        "parallelism": f"work partition x{world} (one tensor stream per GPU)",
                        "l2": "lattices (3 x 19 x 0.94 M pores x elem: 215 MB fp32, 108 MB fp16) stream from HBM "
                              "every step; inputs are the whole tensor solve, not a cached kernel"},

@@ -18,7 +18,7 @@ LBM_VARIANT_DEFAULT = -1      # the library's per-precision default step-kernel 
 FP64, FP32, FP16, BF16, M32, M64, MD32 = 0, 1, 2, 3, 4, 5, 6
 PRECISIONS = {"fp64": FP64, "fp32": FP32, "fp16": FP16, "bf16": BF16, "m32": M32, "m64": M64,
               "md32": MD32}
-CRIT_DRIFT, CRIT_BLOCK = 0, 1
+CRIT_DRIFT, CRIT_BLOCK, CRIT_BATCH = 0, 1, 2
 
 # Exported symbols, exactly those include/lbm.h declares.
 SYMBOLS = (

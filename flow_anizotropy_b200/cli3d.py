@@ -11,7 +11,7 @@ Exit 0 = all three converged, 3 = a direction did not (row still written),
 Options beyond the reference's (all default to the reference's behaviour):
   --tau T            relaxation time (reference: compile-time 1.0)
   --precision P      fp64 (default, the reference's arithmetic) | fp32 | fp16 | bf16
-  --criterion C      drift (reference) | block (block means + k-sigma) | auto
+  --criterion C      drift (reference) | block (block means + k-sigma) | batch (block, batch-means SE) | auto
   --device N         CUDA device
 """
 from __future__ import annotations
@@ -46,7 +46,7 @@ appends one row with the full 3x3 permeability tensor to <results.csv>.
   --quiet           suppress per-check progress
   --tau T           relaxation time                          (default 1)
   --precision P     fp64 | fp32 | fp16 | bf16                (default fp64)
-  --criterion C     drift | block | auto                     (default auto)
+  --criterion C     drift | block | batch | auto             (default auto)
   --device N        CUDA device                              (default 0)
 """
 
@@ -117,7 +117,7 @@ def parse(argv):
         i += 1
     if cfg["precision"] not in ("fp64", "fp32", "fp16", "bf16", "m32", "m64", "md32"):
         raise Die("unknown precision " + cfg["precision"])
-    if cfg["criterion"] not in ("drift", "block", "auto"):
+    if cfg["criterion"] not in ("drift", "block", "batch", "auto"):
         raise Die("unknown criterion " + cfg["criterion"])
     return structure, resultfile, cfg
 

@@ -162,8 +162,9 @@ int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
     if (p.precision < LBM_FP64 || p.precision > LBM_MD32) return lbm_fail_input(ctx, "unknown precision");
     if ((is_moment(p.precision) || is_dense_m(p.precision)) && p.tau != 1.0)
         return lbm_fail_input(ctx, "moment-projected storage needs tau = 1");
-    if (p.criterion != LBM_CRIT_DRIFT && p.criterion != LBM_CRIT_BLOCK) return lbm_fail_input(ctx, "unknown criterion");
-    if (p.criterion == LBM_CRIT_BLOCK && (p.sample <= 0 || p.lag % p.sample != 0))
+    if (p.criterion != LBM_CRIT_DRIFT && p.criterion != LBM_CRIT_BLOCK && p.criterion != LBM_CRIT_BATCH)
+        return lbm_fail_input(ctx, "unknown criterion");
+    if (p.criterion != LBM_CRIT_DRIFT && (p.sample <= 0 || p.lag % p.sample != 0))
         return lbm_fail_input(ctx, "block criterion needs sample > 0 dividing lag");
     if (p.variant != LBM_VARIANT_DEFAULT && (p.variant < 0 || p.variant >= variant_count(p.precision)))
         return lbm_fail_input(ctx, "unknown step-kernel variant");

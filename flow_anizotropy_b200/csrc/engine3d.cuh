@@ -69,9 +69,9 @@ struct Ctl3 {
     double eps;
     long long lag, min_steps, max_steps, avg_steps;
     int hold;
-    int criterion;        // 0: instantaneous drift (reference); 1: block means
-    long long sample;     // criterion 1: flux sample interval
-    double ksigma;        // criterion 1: k-sigma acceptance
+    int criterion;        // 0: instantaneous drift (reference); 1: block means; 2: block means, batch-means SE
+    long long sample;     // criteria 1-2: flux sample interval
+    double ksigma;        // criteria 1-2: k-sigma acceptance
 };
 
 enum { PH_RUN = 1, PH_AVG = 2, PH_DONE = 3, PH_ERR = 4 };
@@ -91,6 +91,8 @@ struct State3 {
     double qprev[3];
     double bs[3], bss[3], pse[3];
     long long bn;
+    double ws[3];         // criterion 2: sum of the current sub-block's samples
+    long long wn;
     double sum[3], sumsq[3];
     long long n_avg;
     double q[3], se[3];
@@ -153,7 +155,7 @@ __device__ __forceinline__ bool needs_reduction(const Ctl3 &c, int phase, long l
     if (phase == PH_AVG) return true;
     if (n == c.max_steps) return true;
     if (n % c.lag == 0) return true;
-    return c.criterion == 1 && (n % c.sample == 0);
+    return c.criterion != 0 && (n % c.sample == 0);
 }
 
 // Controller step, run by one thread once the flux q of step n is known.
@@ -180,8 +182,22 @@ __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const
             if (n % c.sample == 0) {
                 for (int k = 0; k < 3; ++k)
                     if (!isfinite(q[k])) { st.status = 2; st.phase = PH_ERR; st.steps = n; return; }
-                for (int k = 0; k < 3; ++k) { st.bs[k] += q[k]; st.bss[k] += q[k] * q[k]; }
-                st.bn++;
+                if (c.criterion == 1) {
+                    for (int k = 0; k < 3; ++k) { st.bs[k] += q[k]; st.bss[k] += q[k] * q[k]; }
+                    st.bn++;
+                } else {
+                    // batch means: a block's SE from the means of its 10 sub-blocks
+                    const long long per = c.lag / c.sample / 10 > 0 ? c.lag / c.sample / 10 : 1;
+                    for (int k = 0; k < 3; ++k) st.ws[k] += q[k];
+                    if (++st.wn == per) {
+                        for (int k = 0; k < 3; ++k) {
+                            const double mb = st.ws[k] / (double)per;
+                            st.bs[k] += mb; st.bss[k] += mb * mb; st.ws[k] = 0.0;
+                        }
+                        st.wn = 0;
+                        st.bn++;
+                    }
+                }
             }
             if (n % c.lag == 0 && st.bn >= 2) {
                 const double bn = (double)st.bn;
@@ -203,9 +219,10 @@ __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const
                 }
                 for (int k = 0; k < 3; ++k) {
                     st.qprev[k] = m[k]; st.pse[k] = se[k];
-                    st.bs[k] = 0.0; st.bss[k] = 0.0;
+                    st.bs[k] = 0.0; st.bss[k] = 0.0; st.ws[k] = 0.0;
                 }
                 st.bn = 0;
+                st.wn = 0;
                 st.have_prev = 1;
             }
         }

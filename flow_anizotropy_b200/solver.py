@@ -35,7 +35,7 @@ class Params3D:
     max_steps: int = 200000
     avg_steps: int = 2000
     precision: str = "fp64"
-    criterion: str = "auto"     # "drift" (reference), "block", or auto: block for fp16/bf16
+    criterion: str = "auto"     # "drift" (reference), "block", "batch", or auto: batch for fp16/bf16
     sample: int = 10
     ksigma: float = 3.0
     variant: int = _lib.LBM_VARIANT_DEFAULT   # or an index from tune3d
@@ -44,8 +44,8 @@ class Params3D:
         prec = _lib.PRECISIONS[self.precision]
         crit = self.criterion
         if crit == "auto":
-            crit = "block" if prec in (_lib.FP16, _lib.BF16) else "drift"
-        crit_code = {"drift": _lib.CRIT_DRIFT, "block": _lib.CRIT_BLOCK}[crit]
+            crit = "batch" if prec in (_lib.FP16, _lib.BF16) else "drift"
+        crit_code = {"drift": _lib.CRIT_DRIFT, "block": _lib.CRIT_BLOCK, "batch": _lib.CRIT_BATCH}[crit]
         return _lib.Params3D(tau=self.tau, eps=self.eps, lag=int(self.lag),
                              min_steps=int(self.min_steps), max_steps=int(self.max_steps),
                              avg_steps=int(self.avg_steps), hold=int(self.hold),

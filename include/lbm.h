@@ -66,6 +66,10 @@ extern "C" {
 #define LBM_CRIT_BLOCK  1  /* block means over lag steps sampled every `sample`
                               steps, accepted within max(eps ||m||, ksigma * SE)
                               (the 2D reference's test, LMB2d/main.cpp:123-178) */
+#define LBM_CRIT_BATCH  2  /* LBM_CRIT_BLOCK with the SE of a block taken from
+                              the means of its 10 sub-blocks (batch means), so
+                              noise correlated over many steps (stochastic
+                              rounding of 16-bit storage) is not underrated   */
 
 typedef struct lbm_ctx lbm_ctx;
 
