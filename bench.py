@@ -266,7 +266,7 @@ def serve_trace(device, prec, args):
                  min_steps=WORKLOAD["min_steps"], max_steps=WORKLOAD["max_steps"],
                  avg_steps=WORKLOAD["avg_steps"], precision=prec)
     forces = [[F, 0, 0], [0, F, 0], [0, 0, F]]
-    srv = Server(precision=prec, hbm_budget=150 * 2**30, chunk=128, device=device)
+    srv = Server(precision=prec, hbm_budget=150 * 2**30, chunk=128, device=device, variant=args.serve_variant)
     arrivals = poisson_arrivals(20.0, args.serve_seconds, seed=11)
     t0 = time.perf_counter()
     stats = replay(srv, arrivals, lambda i: (pool[i % len(pool)], forces, p))
@@ -290,7 +290,8 @@ def serve_trace(device, prec, args):
             "k_tensors_per_hr": 3600.0 * served, "served_per_s": served, "overloaded": 20.0 > served,
             "plain_fp32_per_s": plain, "speedup_vs_plain_fp32": served / plain,
             "admission": f"FIFO, HBM budget 150 GiB, resident work cap {srv.max_work} pore-voxel-directions",
-            "mix": "batch mix, edges 48 and 64 only (8 seeded structures, reused)", "path": prec}
+            "mix": "batch mix, edges 48 and 64 only (8 seeded structures, reused)", "path": prec,
+            "batch_variant": args.serve_variant}
 
 
 # -------------------------------------------------------------- our arm ----
@@ -384,8 +385,6 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg_bytes / (head["ms"] / 1e3) / 1e9
     per_launch_alg = alg_bytes / max(1, head["launches"])
     traffic = profiled_traffic(head_prec)
-    # served in FP32: on the small serving structures FP16 needs up to 6x the
-    # steps under its criterion (measured 42000 against 7000), so FP32 serves more
     serving = serve_trace(device, args.serve_precision, args) if args.serve_seconds > 0 else None
     out = None
     if rank == 0:
@@ -664,7 +663,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32", "md32"])
     ap.add_argument("--serve-seconds", type=float, default=5.0)
-    ap.add_argument("--serve-precision", default="fp32", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--serve-precision", default="fp16", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--serve-variant", type=int, default=1,
+                    help="step-kernel variant of the serving batch (-1: library default; 1 measured "
+                         "fastest for FP16 on the 48^3-64^3 serving mix)")
     ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch", "gen3d", "large", "perm2d"])
     ap.add_argument("--group2d", type=int, default=16, help="images per launch of the perm2d workload")
     ap.add_argument("--large-n", type=int, default=512, help="cell edge of the large workload")
