@@ -9,6 +9,7 @@ buffers; their pointers are passed straight through).
 from __future__ import annotations
 
 import ctypes as C
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -36,7 +37,7 @@ class Params3D:
     avg_steps: int = 2000
     precision: str = "fp64"
     criterion: str = "auto"     # "drift" (reference), "block", "batch", or auto: batch for fp16/bf16
-    sample: int = 10
+    sample: int = 50            # block criteria: flux sampled every `sample` steps (gcd with lag if it does not divide it)
     ksigma: float = 3.0
     variant: int = _lib.LBM_VARIANT_DEFAULT   # or an index from tune3d
 
@@ -50,7 +51,15 @@ class Params3D:
                              min_steps=int(self.min_steps), max_steps=int(self.max_steps),
                              avg_steps=int(self.avg_steps), hold=int(self.hold),
                              precision=prec, criterion=crit_code, variant=int(self.variant),
-                             sample=int(self.sample), ksigma=float(self.ksigma))
+                             sample=_sample_for(int(self.lag), int(self.sample)), ksigma=float(self.ksigma))
+
+
+def _sample_for(lag: int, sample: int) -> int:
+    """The sample interval of the block criteria must divide lag: the largest
+    common divisor of the two when `sample` does not."""
+    if sample <= 0 or lag <= 0:
+        return sample
+    return sample if lag % sample == 0 else math.gcd(lag, sample)
 
 
 @dataclass

@@ -248,3 +248,13 @@ def test_batch3d_plan_resume_and_atomic_rows(tmp_path):
     assert [t.sample_id for t in cached] == [0]
     assert [t.sample_id for t in work] == [1, 2, 3, 4]
     assert not Path(tasks[1].out_csv).exists()
+
+
+def test_block_criterion_sample_divides_lag():
+    from flow_anizotropy_b200 import solver as S
+    assert S.Params3D(lag=1000, precision="fp16").to_c().sample == 50
+    assert S.Params3D(lag=120, precision="fp16").to_c().sample == 10      # gcd(120, 50)
+    assert S.Params3D(lag=7, sample=3, precision="fp16").to_c().sample == 1
+    for lag in (100, 120, 250, 333, 1000, 2000):
+        s = S.Params3D(lag=lag).to_c().sample
+        assert s > 0 and lag % s == 0
