@@ -46,7 +46,8 @@ appends one row with the full 3x3 permeability tensor to <results.csv>.
   --quiet           suppress per-check progress
   --tau T           relaxation time                          (default 1)
   --precision P     fp64 | fp32 | fp16 | bf16                (default fp64)
-  --criterion C     drift | block | batch | auto             (default auto)
+  --criterion C     drift | block | batch | auto             (default auto:
+                    drift for fp64/fp32, batch for fp16/bf16)
   --device N        CUDA device                              (default 0)
 """
 
