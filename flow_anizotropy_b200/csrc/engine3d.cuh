@@ -269,7 +269,9 @@ __device__ __forceinline__ void cta_sync()
 }
 
 // Block-wide fixed-order sum of three doubles; result valid in thread 0.
-template <int NT = TPB, int BAR = 0>
+// TRAIL = false leaves out the closing barrier: the caller then has one
+// before any thread can write `sh` again.
+template <int NT = TPB, int BAR = 0, bool TRAIL = true>
 __device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
 {
 #pragma unroll
@@ -284,7 +286,7 @@ __device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
         for (int w = 0; w < NT / 32; ++w) { a0 += sh[w][0]; a1 += sh[w][1]; a2 += sh[w][2]; }
         v[0] = a0; v[1] = a1; v[2] = a2;
     }
-    cta_sync<NT, BAR>();
+    if constexpr (TRAIL) cta_sync<NT, BAR>();
 }
 
 // Tile finished on a reduction step: publish the tile's flux partial; the
@@ -296,7 +298,7 @@ __device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long
                                             double (&acc)[3], double (*sh)[3])
 {
     __shared__ int s_last;
-    block_sum3<NT, BAR>(acc, sh);
+    block_sum3<NT, BAR, false>(acc, sh);    // the s_last barrier below closes it
     if (threadIdx.x == 0) {
         double *p = S.partials + 3ll * tile;
         p[0] = acc[0]; p[1] = acc[1]; p[2] = acc[2];
