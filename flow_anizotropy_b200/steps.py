@@ -30,6 +30,8 @@ def main(argv=None):
     ap.add_argument("--variant", type=int, default=-1, help="step-kernel variant (-1: autotune)")
     ap.add_argument("--steps", type=int, default=24)
     ap.add_argument("--tau", type=float, default=1.0)
+    ap.add_argument("--lag", type=int, default=10**9,
+                    help="reduce the flux every LAG steps (1: every step, as in the averaging phase)")
     ap.add_argument("--images", type=int, default=0,
                     help="D2Q9 instead: this many 256^2 disc packings, both directions, one launch per step")
     a = ap.parse_args(argv)
@@ -45,7 +47,7 @@ def main(argv=None):
     if variant < 0:
         variant, _ = S.tune3d(solid, ndir=3, precision=a.precision, nsteps=50)
     F = 1e-6
-    p = S.Params3D(precision=a.precision, criterion="drift", tau=a.tau, lag=10**9, max_steps=a.steps,
+    p = S.Params3D(precision=a.precision, criterion="drift", tau=a.tau, lag=a.lag, max_steps=a.steps,
                    avg_steps=0, hold=10**6, variant=variant)
     runs, rc, _ = S.solve3d(solid, [[F, 0, 0], [0, F, 0], [0, 0, F]], p)
     for r in runs:
