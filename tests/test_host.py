@@ -79,6 +79,10 @@ def test_cli3d_parse():
         parse(["a.raw", "b.csv", "--bogus"])
     with pytest.raises(Die, match="missing value for --lag"):
         parse(["a.raw", "b.csv", "--lag"])
+    for crit in ("drift", "block", "batch", "auto"):
+        assert parse(["a.raw", "b.csv", "--criterion", crit])[2]["criterion"] == crit
+    with pytest.raises(Die, match="unknown criterion"):
+        parse(["a.raw", "b.csv", "--criterion", "median"])
 
 
 def test_cli_exit_codes(tmp_path):
@@ -258,3 +262,15 @@ def test_block_criterion_sample_divides_lag():
     for lag in (100, 120, 250, 333, 1000, 2000):
         s = S.Params3D(lag=lag).to_c().sample
         assert s > 0 and lag % s == 0
+
+
+def test_criterion_codes():
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200 import solver as S
+    assert S.Params3D(precision="fp16").to_c().criterion == _lib.CRIT_BATCH
+    assert S.Params3D(precision="bf16").to_c().criterion == _lib.CRIT_BATCH
+    assert S.Params3D(precision="fp32").to_c().criterion == _lib.CRIT_DRIFT
+    assert S.Params3D(precision="fp64").to_c().criterion == _lib.CRIT_DRIFT
+    assert S.Params3D(precision="fp16", criterion="block").to_c().criterion == _lib.CRIT_BLOCK
+    assert S.Params3D(precision="fp32", criterion="batch").to_c().criterion == _lib.CRIT_BATCH
+    assert S.Params3D().to_c().variant == _lib.LBM_VARIANT_DEFAULT
