@@ -24,33 +24,50 @@ class StructureError(ValueError):
     """Input the reference solver would reject with exit code 2."""
 
 
+_HDR = np.dtype("<i4")
+
+
+def _encode(solid) -> bytes:
+    """Header + payload bytes of a [z, y, x] array of {0, 1}."""
+    vox = np.asarray(solid)
+    if vox.ndim != 3:
+        raise ValueError(f"a .raw structure is 3D [z, y, x]; got an array of shape {vox.shape}")
+    vox = vox.astype(np.uint8, copy=False)
+    if vox.size and int(vox.max()) > 1:
+        raise ValueError("voxel values must be 0 (pore) or 1 (solid)")
+    dims = np.array(vox.shape[::-1], dtype=_HDR)          # nx, ny, nz
+    return dims.tobytes() + np.ascontiguousarray(vox).tobytes()
+
+
+def _decode(buf: bytes, where: str) -> np.ndarray:
+    """[z, y, x] view of header + payload; ValueError when the sizes disagree."""
+    if len(buf) < MAGIC_HEADER_BYTES:
+        raise ValueError(f"{where}: {len(buf)} bytes, fewer than the {MAGIC_HEADER_BYTES}-byte header")
+    nx, ny, nz = (int(d) for d in np.frombuffer(buf[:MAGIC_HEADER_BYTES], dtype=_HDR))
+    payload = len(buf) - MAGIC_HEADER_BYTES
+    if min(nx, ny, nz) < 0 or nx * ny * nz != payload:
+        raise ValueError(f"{where}: dimensions {nx} x {ny} x {nz} do not match the "
+                         f"{payload}-byte payload")
+    return np.frombuffer(buf, dtype=np.uint8, offset=MAGIC_HEADER_BYTES).reshape(nz, ny, nx)
+
+
 def save_structure(path, solid) -> Path:
-    """Write a (nz, ny, nx) {0,1} array as .raw (scripts/structure_io3d.py:40-52)."""
-    solid = np.ascontiguousarray(solid).astype(np.uint8)
-    if solid.ndim != 3:
-        raise ValueError(f"expected a 3D array, got shape {solid.shape}")
-    if solid.size and solid.max() > 1:
-        raise ValueError("structure must be binary (0 = pore, 1 = solid)")
-    nz, ny, nx = solid.shape
+    """Write a [z, y, x] array of {0, 1} (1 = solid) as a .raw file; returns the path.
+
+    Same contract as the reference's writer (scripts/structure_io3d.py:40-52):
+    ValueError for a non-3D or non-binary array."""
     path = Path(path)
-    with open(path, "wb") as fh:
-        fh.write(np.array([nx, ny, nz], dtype="<i4").tobytes())
-        fh.write(solid.tobytes())
+    path.write_bytes(_encode(solid))
     return path
 
 
 def load_structure(path) -> np.ndarray:
-    """Read a .raw as uint8 (nz, ny, nx) (scripts/structure_io3d.py:55-67)."""
+    """Read a .raw file as a read-only uint8 [z, y, x] array (1 = solid).
+
+    Same contract as the reference's reader (scripts/structure_io3d.py:55-67):
+    ValueError when the header's shape does not match the file size."""
     path = Path(path)
-    raw = path.read_bytes()
-    if len(raw) < MAGIC_HEADER_BYTES:
-        raise ValueError(f"{path}: too short to hold a header")
-    nx, ny, nz = (int(v) for v in np.frombuffer(raw, dtype="<i4", count=3))
-    expect = MAGIC_HEADER_BYTES + nx * ny * nz
-    if len(raw) != expect:
-        raise ValueError(
-            f"{path}: header says {nx}x{ny}x{nz} -> {expect} bytes, file has {len(raw)}")
-    return np.frombuffer(raw, dtype=np.uint8, offset=MAGIC_HEADER_BYTES).reshape(nz, ny, nx)
+    return _decode(path.read_bytes(), str(path))
 
 
 def porosity(solid) -> float:
