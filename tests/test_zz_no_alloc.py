@@ -7,6 +7,7 @@ every other GPU test of the session (with the allocator pools of the earlier
 tests warm); run alone, they pass in a fresh process as well.
 """
 import ctypes as C
+import ctypes.util
 import re
 from pathlib import Path
 
@@ -122,3 +123,40 @@ def test_limits_rejected(gpu):
     assert rc == _lib.LBM_EINPUT and "non-binary" in gpu.error()
     # a rejected call leaves the scratch usable
     _assert_same(_call(gpu, "lbm_solve2d_noalloc", ok), _call(gpu, "lbm_solve2d", ok))
+
+
+def _pool_bytes(device):
+    """(reserved, used) bytes of the device's default stream-ordered pool, the
+    pool the library's other entry points allocate from (driver API, so it is
+    the same pool whichever CUDA runtime copy asked for it)."""
+    cu = C.CDLL(ctypes.util.find_library("cuda") or "libcuda.so.1")
+    dev = C.c_int()
+    assert cu.cuDeviceGet(C.byref(dev), device) == 0
+    pool = C.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(C.byref(pool), dev) == 0
+    out = []
+    for attr in (5, 7):     # CU_MEMPOOL_ATTR_RESERVED_MEM_CURRENT, CU_MEMPOOL_ATTR_USED_MEM_CURRENT
+        v = C.c_uint64()
+        assert cu.cuMemPoolGetAttribute(pool, attr, C.byref(v)) == 0
+        out.append(v.value)
+    return tuple(out)
+
+
+@pytest.mark.gpu
+def test_second_call_allocates_nothing(gpu):
+    """After a first call (which may load the module and its static array),
+    a second call changes neither the device's free memory nor the default
+    pool's reserved or used bytes, and gives the same results."""
+    import torch
+    solid = _solid((96, 80), 13, 0.25)
+    first = _call(gpu, "lbm_solve2d_noalloc", solid)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    pool0 = _pool_bytes(0)
+    second = _call(gpu, "lbm_solve2d_noalloc", solid)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    pool1 = _pool_bytes(0)
+    assert free1 == free0, (free0, free1)
+    assert pool1 == pool0, (pool0, pool1)
+    _assert_same(second, first)
