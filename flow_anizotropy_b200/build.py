@@ -30,6 +30,7 @@ UNITS = {
     "k3d_lp.cu": [],
     "k3d_m.cu": [],
     "k3d_md.cu": [],
+    "k3d_reduce.cu": [],
     "engine.cu": [],
     "engine2.cu": [],
     "engine2_noalloc.cu": [],

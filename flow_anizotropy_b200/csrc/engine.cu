@@ -215,6 +215,7 @@ int lbm_effective_variant(int prec, int variant, bool have_meta)
     if (is_moment(prec) || is_dense_m(prec) || have_meta) return variant;
     const int ve = variant % nvar_even(prec);
     if (!even_meta(ve)) return variant;
+    if (even_links(ve)) return variant - ve + 10;       // grouped link slots (one voxel at a time), ranks from the mask
     if (even_grouped(ve)) return variant - ve + 6;      // grouped, ranks from the mask
     return variant - ve + (ve & 1) + 2;                 // same budget, ranks from the mask
 }
@@ -394,6 +395,17 @@ void lbm_copy_pores(Solve3 &dst, const Solve3 &src)
 // numbers and kernels are those of single launches.
 constexpr int kGraphSteps3 = 64;
 
+// Does a solve of this precision reduce its flux through deferred slots (its
+// partials buffer then holds DEFER_SLOTS x ntiles x 3 doubles)?  The dense
+// moment form keeps the immediate reduction (its tiles have their own block
+// size).
+bool lbm_defers(int prec) { return !is_dense_m(prec); }
+
+long long lbm_partial_doubles(int prec, int ntiles)
+{
+    return 3ll * ntiles * (lbm_defers(prec) ? DEFER_SLOTS : 1);
+}
+
 static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, State3 *d_states,
                        const int2 *d_work, int nwork, int prec, int variant, std::vector<State3> &hst)
 {
@@ -402,8 +414,15 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
     for (const Solve3 &S : hs) w1 = w1 && S.P.tau == 1.0;
     variant = lbm_effective_variant(prec, variant, hs.empty() || hs[0].meta != nullptr);
     long long s = 0, base = 0;        // steps done; s_base of the unfinished solves (host copy)
+    const bool defer = lbm_defers(prec);
+    DevMem qbuf(ctx->stream);
+    if (defer) CK(qbuf.alloc(sizeof(double) * 4 * DEFER_SLOTS * (size_t)std::max(1, n)));
+    double *qb = static_cast<double *>(qbuf.p);
+    long long pend0 = 0;              // deferred single launches not yet reduced: [pend0, pend0 + pending)
+    int pending = 0;
     StepArgs a;
     a.solves = d_solves; a.work = d_work; a.nwork_dev = nullptr; a.nwork = nwork;
+    a.defer = defer ? 1 : 0;
     StepArgs ae = a;                  // even steps (grouped work list for grouped variants)
     DevMem gwork(ctx->stream);
     if (lbm_grouped_variant(prec, variant)) {
@@ -430,6 +449,14 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
         x.step = rel;
         return lbm_launch_step(prec, variant, w1, odd, dim3(x.nwork), ctx->stream, x);
     };
+    // reduce and control the deferred single launches (before s_base moves,
+    // before a chunk reuses their slots, and before the states are read)
+    auto flush = [&]() -> cudaError_t {
+        if (!pending) return cudaSuccess;
+        const cudaError_t e = launch_deferred3d(d_solves, n, pend0, pending, qb, ctx->stream);
+        pending = 0;
+        return e;
+    };
     for (;;) {
         CK(cudaMemcpyAsync(hst.data(), d_states, sizeof(State3) * n, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -451,6 +478,7 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
             cudaError_t e = cudaSuccess;
             // launch i of a chunk runs step i + 1 after s_base (s_base even)
             for (int i = 0; i < kGraphSteps3 && e == cudaSuccess; ++i) e = launch(i, ((i + 1) & 1) == 1);
+            if (e == cudaSuccess && defer) e = launch_deferred3d(d_solves, n, 0, kGraphSteps3, qb, ctx->stream);
             if (e == cudaSuccess) {
                 advance3d_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(d_solves, n, kGraphSteps3);
                 e = cudaGetLastError();
@@ -462,6 +490,7 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
         }
         while (s < target) {
             if (exec && (s & 1) == 0 && target - s >= kGraphSteps3) {
+                CK(flush());
                 if (base != s) {
                     // a chunk numbers its steps from s_base: catch up with the single steps
                     advance3d_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(d_solves, n, s - base);
@@ -474,9 +503,14 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
             } else {
                 // every unfinished solve of the call is at step s + 1 (they start together)
                 CK(launch(s - base, ((s + 1) & 1) == 1));
+                if (defer) {
+                    if (!pending) pend0 = s - base;
+                    if (++pending == DEFER_SLOTS) CK(flush());
+                }
                 ++s;
             }
         }
+        CK(flush());
     }
     return LBM_OK;
 }
@@ -522,7 +556,7 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
         lat.emplace_back(ctx->stream);
         part.emplace_back(ctx->stream);
         CK(lat.back().alloc((size_t)lbm_lattice_bytes(S)));
-        CK(part.back().alloc(sizeof(double) * 3 * (size_t)S.ntiles));
+        CK(part.back().alloc(sizeof(double) * (size_t)lbm_partial_doubles(prec, S.ntiles)));
         S.A = lat.back().p;
         S.mask = static_cast<const uint32_t *>(mask.p);
         S.partials = static_cast<double *>(part.back().p);
@@ -622,7 +656,7 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     rc = lbm_build_pores(ctx, S, npt, wpre, fnode, meta, meta2);
     if (rc) return rc;
     CK(lat.alloc((size_t)lbm_lattice_bytes(S)));
-    CK(part.alloc(sizeof(double) * 3 * (size_t)S.ntiles));
+    CK(part.alloc(sizeof(double) * (size_t)lbm_partial_doubles(precision, S.ntiles)));
     CK(d_states.alloc(sizeof(State3)));
     S.A = lat.p; S.mask = static_cast<const uint32_t *>(mask.p);
     S.partials = static_cast<double *>(part.p); S.st = static_cast<State3 *>(d_states.p);

@@ -142,7 +142,17 @@ struct StepArgs {
     long long step;       // steps completed = st->s_base + step
     unsigned long long wait_ns = 0;   // bulk-staged kernels: wait limit (0: WAIT_NS)
     int starve = 0;                   // test only: the bulk producer issues nothing
+    int defer = 0;                    // flux partials to deferred slots (see finish_tile)
 };
+
+// Deferred reduction: with StepArgs::defer set, a reduction step leaves each
+// tile's flux partial in slot (step & (DEFER_SLOTS - 1)) of the solve's
+// partials (DEFER_SLOTS x ntiles x 3 doubles), and reduce3d_kernel /
+// control3d_kernel sum and control those steps, in step order, after at most
+// DEFER_SLOTS launches.  The host launches them before the controller's phase
+// can matter again (every lag multiple, every phase end), so the step kernels
+// of a reduction step need no fence, ticket or last-tile pass.
+constexpr int DEFER_SLOTS = 64;
 
 // ----------------------------------------------------------------- helpers --
 __device__ __forceinline__ int mbit(const uint32_t *row, int x)
@@ -161,7 +171,19 @@ __device__ __forceinline__ bool needs_reduction(const Ctl3 &c, int phase, long l
 // Controller step, run by one thread once the flux q of step n is known.
 // Phase 1 is LMB3d/lbm3d-perm.cpp:332-364 (criterion 0), or the block-mean
 // test of LMB2d/main.cpp:123-178 on 3D flux vectors (criterion 1); phase 2 is
-// the averaging of :370-390.
+// the averaging of :370-390.  Every FP64 operation is written with its
+// rounding (no contraction left to the compiler), so the controller gives
+// the same bits in every translation unit that runs it: in the step kernels
+// of any precision and in the deferred reduction kernel.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dnorm3(const double v[3])
+{
+    return __dsqrt_rn(dadd(dadd(dmul(v[0], v[0]), dmul(v[1], v[1])), dmul(v[2], v[2])));
+}
+
 __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const double q[3])
 {
     if (st.phase == PH_RUN) {
@@ -170,10 +192,10 @@ __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const
             if (n % c.lag == 0) {
                 for (int k = 0; k < 3; ++k)
                     if (!isfinite(q[k])) { st.status = 2; st.phase = PH_ERR; st.steps = n; return; }
-                const double norm = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                const double norm = dnorm3(q);
                 double drift = 0.0;
-                for (int k = 0; k < 3; ++k) drift = fmax(drift, fabs(q[k] - st.qprev[k]));
-                if (st.have_prev && n >= c.min_steps && drift < c.eps * norm) st.hold++;
+                for (int k = 0; k < 3; ++k) drift = fmax(drift, fabs(dsub(q[k], st.qprev[k])));
+                if (st.have_prev && n >= c.min_steps && drift < dmul(c.eps, norm)) st.hold++;
                 else st.hold = 0;
                 for (int k = 0; k < 3; ++k) st.qprev[k] = q[k];
                 st.have_prev = 1;
@@ -183,16 +205,16 @@ __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const
                 for (int k = 0; k < 3; ++k)
                     if (!isfinite(q[k])) { st.status = 2; st.phase = PH_ERR; st.steps = n; return; }
                 if (c.criterion == 1) {
-                    for (int k = 0; k < 3; ++k) { st.bs[k] += q[k]; st.bss[k] += q[k] * q[k]; }
+                    for (int k = 0; k < 3; ++k) { st.bs[k] = dadd(st.bs[k], q[k]); st.bss[k] = dadd(st.bss[k], dmul(q[k], q[k])); }
                     st.bn++;
                 } else {
                     // batch means: a block's SE from the means of its 10 sub-blocks
                     const long long per = c.lag / c.sample / 10 > 0 ? c.lag / c.sample / 10 : 1;
-                    for (int k = 0; k < 3; ++k) st.ws[k] += q[k];
+                    for (int k = 0; k < 3; ++k) st.ws[k] = dadd(st.ws[k], q[k]);
                     if (++st.wn == per) {
                         for (int k = 0; k < 3; ++k) {
-                            const double mb = st.ws[k] / (double)per;
-                            st.bs[k] += mb; st.bss[k] += mb * mb; st.ws[k] = 0.0;
+                            const double mb = ddiv(st.ws[k], (double)per);
+                            st.bs[k] = dadd(st.bs[k], mb); st.bss[k] = dadd(st.bss[k], dmul(mb, mb)); st.ws[k] = 0.0;
                         }
                         st.wn = 0;
                         st.bn++;
@@ -203,17 +225,17 @@ __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const
                 const double bn = (double)st.bn;
                 double m[3], se[3];
                 for (int k = 0; k < 3; ++k) {
-                    m[k] = st.bs[k] / bn;
-                    const double v = (st.bss[k] - bn * m[k] * m[k]) / (bn - 1.0);
-                    se[k] = sqrt(fmax(v, 0.0) / bn);
+                    m[k] = ddiv(st.bs[k], bn);
+                    const double v = ddiv(dsub(st.bss[k], dmul(dmul(bn, m[k]), m[k])), dsub(bn, 1.0));
+                    se[k] = __dsqrt_rn(ddiv(fmax(v, 0.0), bn));
                 }
                 if (st.have_prev) {
-                    const double norm = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+                    const double norm = dnorm3(m);
                     bool pass = n >= c.min_steps;
                     for (int k = 0; k < 3; ++k) {
-                        const double tol = fmax(c.eps * norm,
-                                                c.ksigma * sqrt(se[k] * se[k] + st.pse[k] * st.pse[k]));
-                        pass = pass && fabs(m[k] - st.qprev[k]) < tol;
+                        const double tol = fmax(dmul(c.eps, norm),
+                                                dmul(c.ksigma, __dsqrt_rn(dadd(dmul(se[k], se[k]), dmul(st.pse[k], st.pse[k])))));
+                        pass = pass && fabs(dsub(m[k], st.qprev[k])) < tol;
                     }
                     if (pass) st.hold++; else st.hold = 0;
                 }
@@ -241,16 +263,16 @@ __device__ inline void controller3(const Ctl3 &c, State3 &st, long long n, const
         return;
     }
     if (st.phase == PH_AVG) {
-        for (int k = 0; k < 3; ++k) { st.sum[k] += q[k]; st.sumsq[k] += q[k] * q[k]; }
+        for (int k = 0; k < 3; ++k) { st.sum[k] = dadd(st.sum[k], q[k]); st.sumsq[k] = dadd(st.sumsq[k], dmul(q[k], q[k])); }
         st.n_avg++;
         if (st.n_avg >= c.avg_steps) {
             const double nn = (double)st.n_avg;
             for (int k = 0; k < 3; ++k) {
-                st.q[k] = st.sum[k] / nn;
+                st.q[k] = ddiv(st.sum[k], nn);
                 st.se[k] = 0.0;
                 if (st.n_avg > 1) {
-                    const double var = (st.sumsq[k] - nn * st.q[k] * st.q[k]) / (nn - 1.0);
-                    st.se[k] = sqrt(fmax(var, 0.0) / nn);
+                    const double var = ddiv(dsub(st.sumsq[k], dmul(dmul(nn, st.q[k]), st.q[k])), dsub(nn, 1.0));
+                    st.se[k] = __dsqrt_rn(ddiv(fmax(var, 0.0), nn));
                 }
             }
             st.steps = n;
@@ -289,15 +311,30 @@ __device__ __forceinline__ void block_sum3(double (&v)[3], double (*sh)[3])
     if constexpr (TRAIL) cta_sync<NT, BAR>();
 }
 
+__device__ __forceinline__ int defer_slot(const StepArgs &a)
+{
+    return a.defer ? (int)(a.step & (DEFER_SLOTS - 1)) : -1;
+}
+
 // Tile finished on a reduction step: publish the tile's flux partial; the
 // last tile of the solve to finish sums all partials in a fixed order (the
 // result does not depend on which blocks ran which tiles, or on what else is
-// in the batch) and runs the controller.
+// in the batch) and runs the controller.  With slot >= 0 the partial goes to
+// that deferred slot instead, and reduce3d_kernel does the rest later with
+// the same sums in the same order, so the results are the same bits.
 template <int NT = TPB, int BAR = 0>
 __device__ __forceinline__ void finish_tile(const Solve3 &S, int tile, long long n,
-                                            double (&acc)[3], double (*sh)[3])
+                                            double (&acc)[3], double (*sh)[3], int slot = -1)
 {
     __shared__ int s_last;
+    if (slot >= 0) {
+        block_sum3<NT, BAR, true>(acc, sh);
+        if (threadIdx.x == 0) {
+            double *p = S.partials + 3ll * ((long long)slot * S.ntiles + tile);
+            p[0] = acc[0]; p[1] = acc[1]; p[2] = acc[2];
+        }
+        return;
+    }
     block_sum3<NT, BAR, false>(acc, sh);    // the s_last barrier below closes it
     if (threadIdx.x == 0) {
         double *p = S.partials + 3ll * tile;
@@ -456,7 +493,7 @@ __device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, const uin
 // (NVAR_EVEN_LP for the reduced-precision storage, which adds the grouped
 // even kernels); lbm_tune3d times them on the actual structure.
 struct Variant { int npt, minb; };
-constexpr int NVAR_ODD = 3, NVAR_ODD_LP = 5, NVAR_EVEN = 6, NVAR_EVEN_LP = 8;
+constexpr int NVAR_ODD = 3, NVAR_ODD_LP = 5, NVAR_EVEN = 6, NVAR_EVEN_LP = 13;
 constexpr int NVAR_LP = NVAR_ODD_LP * NVAR_EVEN_LP, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
 constexpr int MAX_GROUP = 3;    // directions per grouped even step
 inline int nvar_even(int prec) { return prec == 0 ? NVAR_EVEN : NVAR_EVEN_LP; }
@@ -470,15 +507,22 @@ __host__ __device__ constexpr Variant odd_lp(int v)
 // even variants: 0-1 read the neighbour record (META), 2-3 compute ranks from
 // the mask, 4-5 read the record and stage their gathers with cp.async, 6-7
 // are grouped (one rank computation for all directions of a structure; 6
-// from the mask, 7 from the record)
+// from the mask, 7 from the record), 8-12 are grouped with the link slots
+// kept in shared memory and the directions stepped one at a time (8-9 from
+// the record, 10 from the mask, 11-12 from the record with a thread's two
+// voxels collided together in packed FP32)
 __host__ __device__ constexpr Variant even_lp(int v)
 {
     return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : v == 2 ? Variant{1, 3} : v == 3 ? Variant{1, 4}
-         : v == 4 ? Variant{1, 4} : v == 5 ? Variant{1, 3} : Variant{1, 2};
+         : v == 4 ? Variant{1, 4} : v == 5 ? Variant{1, 3} : v <= 7 ? Variant{1, 2}
+         : v == 8 ? Variant{1, 3} : v == 9 ? Variant{1, 4} : v == 10 ? Variant{1, 3}
+         : v == 11 ? Variant{2, 3} : Variant{2, 2};
 }
-__host__ __device__ constexpr bool even_meta(int v) { return v < 2 || v == 4 || v == 5 || v == 7; }
+__host__ __device__ constexpr bool even_meta(int v) { return v < 2 || v == 4 || v == 5 || v == 7 || v == 8 || v == 9 || v >= 11; }
 __host__ __device__ constexpr bool even_async(int v) { return v == 4 || v == 5; }
 __host__ __device__ constexpr bool even_grouped(int v) { return v >= 6; }
+__host__ __device__ constexpr bool even_links(int v) { return v >= 8; }
+__host__ __device__ constexpr bool even_pair(int v) { return v >= 11; }
 __host__ __device__ constexpr Variant odd_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{2, 1} : Variant{1, 1}; }
 __host__ __device__ constexpr Variant even_f64(int v)
 {
@@ -606,7 +650,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
                 }
             }
         }
-        if (red) finish_tile(S, item.y, n, acc, sh);
+        if (red) finish_tile(S, item.y, n, acc, sh, defer_slot(a));
     }
 }
 
@@ -675,17 +719,32 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepAr
         }
         if (red) {
             canonical_acc<TPB, 0>(su, u, threadIdx.x, ts, (unsigned)S.nfluid, acc);
-            finish_tile(S, item.y, n, acc, sh);
+            finish_tile(S, item.y, n, acc, sh, defer_slot(a));
         }
     }
 }
+
+// What a consumer of the bulk-staged odd step needs to know about its tile,
+// written to shared memory by the producer with the tile's copies, so that
+// the consumers read no global memory before their stores: the item, the
+// solve, its lattice, the step number and reduction flag of this step, and
+// the collision constants.
+struct BulkTile {
+    void *A;
+    long long n;
+    int item, solve, red;
+    unsigned tile_start;     // rank of the tile's first voxel
+    unsigned P, nfluid;
+    float scale, inv_scale;
+    Phys3 phys;
+};
 
 // Odd (local) step staged through shared memory by the copy engine.  A
 // producer warp (the block's last 32 threads; one lane works) walks the work
 // list (persistent grid, stride gridDim.x), skips items of finished solves,
 // and for each tile (TPB * TILE_NPT voxels) issues 19 untiled bulk copies,
 // one per plane run, into a ring of ODD_BULK_STAGES tile buffers; each
-// buffer carries its item index.  The TPB consumer threads collide a tile
+// buffer carries its tile descriptor (BulkTile).  The TPB consumer threads collide a tile
 // out of shared memory (two adjacent voxels per thread, packed, as the pair
 // kernel), store it straight to global memory and release the buffer.  So
 // the loads of the next tiles are in flight while a tile is collided, and
@@ -714,7 +773,7 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
     constexpr int BAR = 1;                               // consumers' named barrier
     extern __shared__ __align__(128) unsigned char ring[];
     __shared__ uint64_t full[NS], empty[NS];
-    __shared__ int slot_item[NS];
+    __shared__ BulkTile slot[NS];
     __shared__ double sh[TPB / 32][3];
     __shared__ float su[3][TPB * TILE_NPT];
     const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
@@ -724,7 +783,7 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
         for (int s = 0; s < NS; ++s) {
             mbar_init(&full[s], 1u);
             mbar_init(&empty[s], (unsigned)TPB);
-            slot_item[s] = -1;
+            slot[s].item = -1;
         }
         mbar_init_fence();
     }
@@ -746,10 +805,12 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
             int w = next;
             unsigned bytes = 0u, P = 0u;
             const T *src = nullptr;
+            BulkTile &d = slot[s];
             for (; w < nwork; w += gridDim.x) {
                 const int2 it = a.work[w];
                 const Solve3 &S = a.solves[it.x];
-                if (S.st->phase >= PH_DONE) continue;
+                const int phase = S.st->phase;
+                if (phase >= PH_DONE) continue;
                 const unsigned i0 = (unsigned)it.y * TV;
                 src = static_cast<const T *>(S.A) + i0;
                 P = (unsigned)S.plane;
@@ -762,11 +823,22 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
                     continue;
                 }
                 bytes = ((unsigned)min(TV, (unsigned)S.nfluid - i0) * (unsigned)sizeof(T) + 15u) & ~15u;
+                const long long n = S.st->s_base + a.step + 1;
+                d.A = S.A;
+                d.n = n;
+                d.tile_start = i0;
+                d.solve = it.x;
+                d.red = needs_reduction(S.c, phase, n) ? 1 : 0;
+                d.P = P;
+                d.nfluid = (unsigned)S.nfluid;
+                d.scale = S.scale;
+                d.inv_scale = S.inv_scale;
+                d.phys = S.P;
                 break;
             }
             const bool more = w < nwork;
             next = more ? w + gridDim.x : w;
-            slot_item[s] = more ? w : -1;
+            d.item = more ? w : -1;
             if (more && bytes) {
                 unsigned char *buf = ring + s * (Q3 * RUN);
                 fence_proxy_async_smem();
@@ -804,7 +876,7 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
                 // the item index is written before the buffer's copies are
                 // issued, so it is there even if they never completed; with
                 // none, the CTA's first item names the solve
-                int w = *static_cast<volatile int *>(&slot_item[s]);
+                int w = *static_cast<volatile int *>(&slot[s].item);
                 if (w < 0 && (int)blockIdx.x < nwork) w = blockIdx.x;
                 if (w >= 0) {
                     const Solve3 &S = a.solves[a.work[w].x];
@@ -816,32 +888,35 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
             return;
         }
         parity ^= 1u << s;
-        const int w = slot_item[s];
+        const BulkTile &d = slot[s];
+        const int w = d.item;
         if (w < 0) break;
-        const int2 item = a.work[w];
-        const Solve3 &S = a.solves[item.x];
-        const long long n = S.st->s_base + a.step + 1;
-        const bool red = needs_reduction(S.c, S.st->phase, n);
-        T *__restrict__ A = static_cast<T *>(S.A);
-        const unsigned P = (unsigned)S.plane;
+        const long long n = d.n;
+        const bool red = d.red != 0;
+        T *__restrict__ A = static_cast<T *>(d.A);
+        const unsigned P = d.P, nf = d.nfluid;
         const T *buf = reinterpret_cast<const T *>(ring + s * (Q3 * RUN));
         double acc[3] = {0.0, 0.0, 0.0};
-        const unsigned ts = (unsigned)item.y * TV;
-        const unsigned i0 = ts + 2u * tid;
         float2 g[Q3], u[3] = {};
 #pragma unroll
         for (int k = 0; k < Q3; ++k) ST::lds2(buf + (k * TV + 2u * tid), g[k].x, g[k].y);
-        mbar_arrive(&empty[s]);    // this thread is done with buffer s
-        if (i0 < (unsigned)S.nfluid) {
-            collide3x2<ST, W1>(g, S, u);
+        const float sc = d.scale, isc = d.inv_scale;
+        const Phys3 phys = d.phys;
+        const int solve = d.solve;
+        const unsigned tstart = d.tile_start;
+        mbar_arrive(&empty[s]);    // this thread is done with buffer s (and its descriptor)
+        const unsigned i0 = tstart + 2u * tid;
+        if (i0 < nf) {
+            collide_pairs<W1, F32x2>(g, phys, sc, isc, u[0], u[1], u[2]);
             const uint32_t h0 = voxel_bits<ST>(i0, n), h1 = voxel_bits<ST>(i0 + 1u, n);
 #pragma unroll
             for (int k = 0; k < Q3; ++k)
                 ST::st2(A + (opp3(k) * P + i0), g[k].x, g[k].y, dir_bits(h0, k), dir_bits(h1, k));
         }
         if (red) {
-            canonical_acc<TPB, BAR>(su, u, tid, ts, (unsigned)S.nfluid, acc);
-            finish_tile<TPB, BAR>(S, item.y, n, acc, sh);
+            const Solve3 &S = a.solves[solve];
+            canonical_acc<TPB, BAR>(su, u, tid, tstart, nf, acc);
+            finish_tile<TPB, BAR>(S, (int)(tstart / TV), n, acc, sh, defer_slot(a));
         }
     }
 }
@@ -911,7 +986,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
-        if (red) finish_tile(S, item.y, n, acc, sh);
+        if (red) finish_tile(S, item.y, n, acc, sh, defer_slot(a));
     }
 }
 
@@ -1004,7 +1079,120 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_group_kernel(const Step
             if (!((redm >> d) & 1u)) continue;
             const Solve3 &S = a.solves[item.x + d];
             double acc[3] = {sacc[d][0][threadIdx.x], sacc[d][1][threadIdx.x], sacc[d][2][threadIdx.x]};
-            finish_tile(S, item.y, S.st->s_base + a.step + 1, acc, sh);
+            finish_tile(S, item.y, S.st->s_base + a.step + 1, acc, sh, defer_slot(a));
+        }
+    }
+}
+
+// Even step of a group of directions that share one structure, with each
+// voxel's 18 link slots found once per step and reused by every direction.
+// The AA even step reads and writes the same slot per link: population k is
+// pulled from slot(o) = A[k][i] across a solid link, else A[o][rank(x - e_k)]
+// (o = opp k), and the post-collision population o is pushed back to that
+// slot.  The slots of the tile's voxels go to shared memory (each thread
+// reads back only its own, so no barrier), then the directions are stepped
+// one after another: a direction costs one shared-memory read and one
+// address computation per access instead of the rank arithmetic and the
+// solid selects, and only one direction's populations are held at a time.
+// Per direction, voxel, step and tile the arithmetic, the random bits and
+// the flux order are those of step3d_even_kernel, so the results are
+// bit-identical to it.  PAIR: a thread's two voxels (t, t + TPB) are pulled
+// together and collided in packed FP32 (the same bits per voxel); a missing
+// second voxel collides zeros and is neither stored nor summed.
+template <class ST, int MINB, bool W1, bool META, bool PAIR>
+__global__ void __launch_bounds__(TPB, MINB) step3d_even_links_kernel(const StepArgs a)
+{
+    static_assert(!PAIR || (ST::shifted && TILE_NPT == 2), "pairs are collided by the packed FP32 operator");
+    using T = typename ST::T;
+    using Cp = typename ST::C;
+    constexpr unsigned TV = TPB * TILE_NPT;
+    __shared__ double sh[TPB / 32][3];
+    __shared__ unsigned sl[Q3 - 1][TV];          // slot of link k (k = 1..18) of each voxel of the tile
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    const unsigned tid = threadIdx.x;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S0 = a.solves[item.x];
+        const int ng = min(S0.group, MAX_GROUP);
+        unsigned live = 0;
+#pragma unroll
+        for (int d = 0; d < MAX_GROUP; ++d)
+            if (d < ng && a.solves[item.x + d].st->phase < PH_DONE) live |= 1u << d;
+        if (!live) continue;
+        const unsigned P = (unsigned)S0.plane;
+        const unsigned nf = (unsigned)S0.nfluid;
+        const unsigned i0 = (unsigned)item.y * TV;
+#pragma unroll
+        for (int j = 0; j < TILE_NPT; ++j) {
+            const unsigned i = i0 + j * TPB + tid;
+            if (i >= nf) continue;
+            CNb nb;
+            if constexpr (META) {
+                meta_nbrs(S0, i, __ldg(S0.meta + i), __ldg(S0.meta2 + i), nb);
+            } else {
+                int x, y, z;
+                coords3(S0, __ldg(S0.fnode + i), x, y, z);
+                compact_nbrs(S0, i, x, y, z, nb);
+            }
+#pragma unroll
+            for (int k = 1; k < Q3; ++k) {
+                const int o = opp3(k);
+                sl[k - 1][j * TPB + tid] = ((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]);
+            }
+        }
+#pragma unroll 1
+        for (int d = 0; d < ng; ++d) {
+            if (!((live >> d) & 1u)) continue;
+            const Solve3 &S = a.solves[item.x + d];
+            const long long n = S.st->s_base + a.step + 1;
+            const bool red = needs_reduction(S.c, S.st->phase, n);
+            T *__restrict__ A = static_cast<T *>(S.A);
+            double acc[3] = {0.0, 0.0, 0.0};
+            if constexpr (PAIR) {
+                const unsigned ia = i0 + tid, ib = i0 + TPB + tid;
+                const bool va = ia < nf, vb = ib < nf;
+                float2 g[Q3], u[3];
+                g[0].x = va ? ST::ld(A + ia) : 0.0f;
+                g[0].y = vb ? ST::ld(A + ib) : 0.0f;
+#pragma unroll
+                for (int k = 1; k < Q3; ++k) {
+                    g[k].x = va ? ST::ld(A + sl[k - 1][tid]) : 0.0f;
+                    g[k].y = vb ? ST::ld(A + sl[k - 1][TPB + tid]) : 0.0f;
+                }
+                collide3x2<ST, W1>(g, S, u);
+                if (va) {
+                    const uint32_t hv = voxel_bits<ST>(ia, n);
+                    store_pop<ST>(A, ia, g[0].x, hv, 0);
+#pragma unroll
+                    for (int k = 1; k < Q3; ++k) store_pop<ST>(A, sl[opp3(k) - 1][tid], g[k].x, hv, k);
+                    acc[0] += (double)u[0].x; acc[1] += (double)u[1].x; acc[2] += (double)u[2].x;
+                }
+                if (vb) {
+                    const uint32_t hv = voxel_bits<ST>(ib, n);
+                    store_pop<ST>(A, ib, g[0].y, hv, 0);
+#pragma unroll
+                    for (int k = 1; k < Q3; ++k) store_pop<ST>(A, sl[opp3(k) - 1][TPB + tid], g[k].y, hv, k);
+                    acc[0] += (double)u[0].y; acc[1] += (double)u[1].y; acc[2] += (double)u[2].y;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < TILE_NPT; ++j) {
+                    const unsigned i = i0 + j * TPB + tid;
+                    if (i >= nf) continue;
+                    Cp g[Q3];
+                    g[0] = ST::ld(A + i);
+#pragma unroll
+                    for (int k = 1; k < Q3; ++k) g[k] = ST::ld(A + sl[k - 1][j * TPB + tid]);
+                    Cp ux, uy, uz;
+                    collide3<ST, W1>(g, S, ux, uy, uz);
+                    const uint32_t hv = voxel_bits<ST>(i, n);
+                    store_pop<ST>(A, i, g[0], hv, 0);
+#pragma unroll
+                    for (int k = 1; k < Q3; ++k) store_pop<ST>(A, sl[opp3(k) - 1][j * TPB + tid], g[k], hv, k);
+                    acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+                }
+            }
+            if (red) finish_tile(S, item.y, n, acc, sh, defer_slot(a));
         }
     }
 }
@@ -1082,7 +1270,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const Step
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
-        if (red) finish_tile(S, item.y, n, acc, sh);
+        if (red) finish_tile(S, item.y, n, acc, sh, defer_slot(a));
     }
 }
 
@@ -1096,6 +1284,12 @@ __global__ void build_meta_kernel(Solve3 S, uint4 *meta, uint2 *meta2);
 
 // After a chunk of `steps` launches, solves still running have advanced by it.
 __global__ void advance3d_kernel(Solve3 *solves, int nsolves, long long steps);
+
+// Deferred reduction of the launches with relative steps step0 .. step0 +
+// nsteps - 1 (nsteps <= DEFER_SLOTS): the fluxes (qbuf: per solve and step,
+// q[3] and a flag), then the controllers in step order.
+cudaError_t launch_deferred3d(const Solve3 *solves, int nsolves, long long step0, int nsteps, double *qbuf,
+                              cudaStream_t s);
 
 // Initial state: every population at rest (f = w, or h = 0 when shifted).
 template <class ST>

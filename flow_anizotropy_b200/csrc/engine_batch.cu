@@ -218,6 +218,9 @@ extern "C" int lbm_batch_set_variant(lbm_batch *b, int variant)
     for (const Slot &s : b->slots)
         if (s.used) return lbm_fail_input(ctx, "the batch has resident solves");
     if (variant_npt(b->precision, variant) != b->npt) return lbm_fail_input(ctx, "variant changes the tile size");
+    if (b->precision >= LBM_FP32 && b->precision <= LBM_BF16 && even_grouped(variant % NVAR_EVEN_LP))
+        return lbm_fail_input(ctx, "grouped even-step variants need a structure's directions in one work item; "
+                                   "the batch steps each direction on its own");
     b->variant = variant;
     b->graph_nwork = -1;      // recapture with the new kernels at the next change
     return LBM_OK;

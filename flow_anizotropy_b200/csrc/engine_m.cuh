@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(TPB, MINB) stepm_kernel(const StepArgs a)
             MT::st(dst, slots, i, c1n, d3n, ux, uy, uz);
             acc3[0] = (double)ux; acc3[1] = (double)uy; acc3[2] = (double)uz;
         }
-        if (red) finish_tile(S, item.y, n, acc3, sh);
+        if (red) finish_tile(S, item.y, n, acc3, sh, defer_slot(a));
     }
 }
 

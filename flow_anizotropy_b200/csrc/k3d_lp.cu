@@ -15,6 +15,7 @@ int max_blocks_f64(int variant, bool odd);
 #define LBM_EVEN(ST, V, W) step3d_even_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 #define LBM_EVENA(ST, V, W) step3d_even_async_kernel<ST, even_lp(V).minb, W>
 #define LBM_EVENG(ST, V, W) step3d_even_group_kernel<ST, even_lp(V).minb, W, even_meta(V)>
+#define LBM_EVENL(ST, V, W) step3d_even_links_kernel<ST, even_lp(V).minb, W, even_meta(V), even_pair(V)>
 #define LBM_ODDB(ST, W) step3d_odd_bulk_kernel<ST, odd_lp(4).minb, W>
 
 // Persistent CTAs of the bulk-staged odd kernel per (storage, tau = 1, device),
@@ -81,7 +82,12 @@ static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const S
         case 4: LBM_EVENA(ST, 4, W)<<<grid, TPB, 0, s>>>(a); break;
         case 5: LBM_EVENA(ST, 5, W)<<<grid, TPB, 0, s>>>(a); break;
         case 6: LBM_EVENG(ST, 6, W)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_EVENG(ST, 7, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 7: LBM_EVENG(ST, 7, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 8: LBM_EVENL(ST, 8, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 9: LBM_EVENL(ST, 9, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 10: LBM_EVENL(ST, 10, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 11: LBM_EVENL(ST, 11, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_EVENL(ST, 12, W)<<<grid, TPB, 0, s>>>(a); break;
         }
     }
     return cudaGetLastError();
@@ -111,7 +117,10 @@ static int occ(int v, bool odd)
                         : (ve == 0 ? (const void *)LBM_EVEN(ST, 0, true) : ve == 1 ? (const void *)LBM_EVEN(ST, 1, true)
                            : ve == 2 ? (const void *)LBM_EVEN(ST, 2, true) : ve == 3 ? (const void *)LBM_EVEN(ST, 3, true)
                            : ve == 4 ? (const void *)LBM_EVENA(ST, 4, true) : ve == 5 ? (const void *)LBM_EVENA(ST, 5, true)
-                           : ve == 6 ? (const void *)LBM_EVENG(ST, 6, true) : (const void *)LBM_EVENG(ST, 7, true));
+                           : ve == 6 ? (const void *)LBM_EVENG(ST, 6, true) : ve == 7 ? (const void *)LBM_EVENG(ST, 7, true)
+                           : ve == 8 ? (const void *)LBM_EVENL(ST, 8, true) : ve == 9 ? (const void *)LBM_EVENL(ST, 9, true)
+                           : ve == 10 ? (const void *)LBM_EVENL(ST, 10, true) : ve == 11 ? (const void *)LBM_EVENL(ST, 11, true)
+                           : (const void *)LBM_EVENL(ST, 12, true));
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
     return nb;

@@ -152,15 +152,19 @@ def poisson_arrivals(rate: float, duration: float, seed: int = 0):
         out.append(t)
 
 
-def replay(server: Server, arrivals, make_request, chunks_per_pump: int = 1):
+def replay(server: Server, arrivals, make_request, chunks_per_pump: int = 1, horizon: float | None = None):
     """Feed requests at their arrival times (seconds from now) while pumping the
-    server; returns the server's stats once every request is done.
+    server; returns the server's stats once every request is done, or, with
+    `horizon`, once that many seconds have passed (requests still queued or
+    resident then are left unfinished: an overloaded server never drains).
     make_request(i) -> (solid, forces, params)."""
     t0 = server.clock()
     i = 0
     n = len(arrivals)
     while i < n or not server.idle():
         now = server.clock() - t0
+        if horizon is not None and now >= horizon:
+            break
         while i < n and arrivals[i] <= now:
             solid, forces, params = make_request(i)
             server.submit(solid, forces, params, t_arrive=t0 + arrivals[i])

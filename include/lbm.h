@@ -177,11 +177,14 @@ int lbm_solve2d_many(lbm_ctx *ctx, int nstruct, const uint8_t *solids, int nx, i
  * (about 7 MB per device, reserved when the library's device code is loaded).
  *   nx * ny > LBM_NOALLOC2D_MAX_CELLS or ndir > LBM_NOALLOC2D_MAX_DIRS:
  * LBM_EINPUT, with lbm_last_error naming the limit.
- *   The first call on a device looks up the array (cudaGetSymbolAddress), which
- * may load the library's device code there: make it before any stream
- * capture.  The call synchronises its stream and is not capturable.
+ *   Every call looks up the array (cudaGetSymbolAddress, so a device reset
+ * between calls is harmless); a device's first call may load the library's
+ * device code there: make it before any stream capture.  The call
+ * synchronises its stream and is not capturable.
  *   One array per device and process: overlapping calls on one device would
- * race on it, so they are serialised by a per-device lock. */
+ * race on it, so they are serialised by a per-device lock.
+ *   The time loop launches one step at a time from the host (about 8.6 us per
+ * step on 256 x 256 against 6.8 us for lbm_solve2d's graph chunks). */
 int lbm_solve2d_noalloc(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny,
                         int ndir, const double *forces, const lbm_params2d *params,
                         lbm_result2d *results, float *vel_out);
@@ -199,7 +202,9 @@ int  lbm_batch_create(lbm_ctx *ctx, lbm_batch **batch, int precision,
 /* Step-kernel variant of every launch of an empty batch (default
  * LBM_VARIANT_DEFAULT, the variant lbm_tune3d picks on the 128^3 tensor
  * workload; mixes of small structures may prefer another).  Results do not
- * depend on it.  LBM_EINPUT while solves are resident. */
+ * depend on it.  LBM_EINPUT while solves are resident, and for the grouped
+ * even-step variants (they step all directions of a structure in one work
+ * item; the batch steps each direction on its own). */
 int  lbm_batch_set_variant(lbm_batch *batch, int variant);
 void lbm_batch_destroy(lbm_batch *batch);
 

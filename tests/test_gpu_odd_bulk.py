@@ -16,7 +16,7 @@ from flow_anizotropy_b200 import structures as st
 
 pytestmark = pytest.mark.gpu
 
-NV_EVEN = 8
+NV_EVEN = 13          # even variants per odd variant (NVAR_EVEN_LP)
 PAIR, BULK = 3, 4          # odd variant indices
 
 
