@@ -4,36 +4,50 @@
 Workload (one bench step = one full permeability tensor): the 128^3 packing
 of overlapping prolate ellipsoids, semi-axes (4, 4, 12) voxels along z,
 porosity 0.45, percolating in x, y and z (seeded, synthetic), solved along
-+x, +y and +z with g = 1e-6 (--ff 4), tau = 1, eps = 1e-6 relative drift every
-1000 steps, hold 2, min 4000, max 50000 steps, 2000 averaging steps.  The
-three directions run concurrently on one GPU.
++x, +y and +z with g = 1e-6 (--ff 4), tau = 1, eps = 1e-6, every 1000 steps,
+hold 2, min 4000, max 50000 steps, 2000 averaging steps.  The three
+directions run concurrently on one GPU.
+
+Stopping rules: FP64 and FP32 storage stop by the reference's rule (relative
+drift of q between checks, LMB3d/lbm3d-perm.cpp:332-364); FP16 and BF16
+storage stop by a block-mean test (the 2D reference's k-sigma test,
+LMB2d/main.cpp:123-178, with batch-means standard errors), because their
+stochastic rounding keeps q wandering at the 1e-6 level the drift test uses.
+Every path's tensor is compared with the FP64 tensor and with the row the
+reference binary wrote for this structure (tests/golden/configs/).
 
 Reported (one JSON line, rank 0):
-  value      k-tensors/hour of the headline path, the fastest of FP32
-             populations, FP16 populations and the tau = 1 FP32 moment forms that
-             stays within 1e-3 of the FP64 tensor (every path keeps the
-             reference's stopping rule), inputs resident in HBM, device time
-             from CUDA events on the solver's stream;
+  value      k-tensors/hour of the headline path: the fastest of FP32, FP16
+             and BF16 storage whose every k_ij is within 1e-3 of FP64; inputs
+             resident in HBM, device time from CUDA events on the solver's
+             stream;
   e2e        the same through the public API with the structure in host memory
              (host->device copy and result read-back inside the timed region);
-  plain_fp32 the same workload with plain FP32 storage, one launch per step;
-  serving    p50/p99 latency of a short 20 requests/s Poisson trace through the
-             continuous-batching server;
-  rel_err    the headline K against the FP64 K of the same structure;
-  roofline   HBM roofline of the step kernel: algorithmic bytes (pore voxels
+  paths      every storage path: k-tensors/h, GLUPS, the 3x3 per-k_ij error
+             matrix against FP64 and against the reference row;
+  mean_velocity  superficial q (the reference's output) and the pore mean
+             q / phi of each forcing direction;
+  serving    the continuous-batching server on the serving mix (batch-mix
+             structures, one 256^3 GRF in every 20 requests) at 20 requests/s
+             for --serve-seconds, p50/p99 latency of what completed;
+  large      512^3 GRF, tau 0.8, fixed steps: GLUPS and roofline per path;
+  batch      a sample of the 256-structure uneven-size mix, batched against
+             one structure at a time in plain FP32;
+  roofline   HBM roofline of the step kernels: algorithmic bytes (pore voxels
              x 2 x 19 x element size + N/8 mask) / time, against the measured
              copy bandwidth;
   cpu_baseline  the reference CPU solver (oracle/_ref/lbm3d-perm, built from
              the reference sources) on all host cores, a bounded fixed-step
-             sample, extrapolated to a converged tensor with the FP64 step
-             counts.
+             sample, extrapolated to a converged tensor with the step counts
+             the reference itself took on this structure.
 
 Multi-GPU (torchrun): every rank solves its own tensors, no collective in the
 data path ("weak" scaling); the timed region is bracketed by a barrier and the
-max over ranks is reported.
+max over ranks is reported.  The serving, large and batch legs run at N = 1.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp16]
     python bench.py --impl reference        # the reference CPU solver alone
+    python bench.py --workload steps --precision fp16 --variant V --steps 12   # profiling runs
 """
 from __future__ import annotations
 
@@ -41,7 +55,6 @@ import argparse
 import json
 import math
 import os
-import re
 import shutil
 import statistics
 import subprocess
@@ -78,12 +91,25 @@ DTYPE = {"fp16": "f16-storage/f32-compute/f64-reduce", "bf16": "bf16-storage/f32
          "fp32": "f32-storage/f32-compute/f64-reduce", "fp64": "f64",
          "m32": "f32 moment records (tau=1)/f32-compute/f64-reduce", "m64": "f64 moment records (tau=1)",
          "md32": "f32 dense moment records (tau=1)/f32-compute/f64-reduce"}
-# Steps per direction of the converged FP64 solve of the workload structure
-# (x, y, z).  Our FP64 path reproduces the reference's step counts exactly
-# (per-step bit-identical populations; see tests/test_gpu_solve3d.py); the
-# reference arm uses these to turn its fixed-step sample into a full tensor.
-FP64_STEPS = (8000, 7000, 8000)
+TAGS = ("fx", "fy", "fz")
+# Row the reference binary appended for the workload structure
+# (tests/golden/make_golden_configs.py); its step counts turn the CPU sample
+# into a converged tensor, and its tensor is the reference every path is
+# compared with.
+REF_ROW = ROOT / "tests" / "golden" / "configs" / "precision128.csv"
 
+
+def reference_row(path=REF_ROW):
+    """Steps, fluxes and K of the reference's row, or None if it is absent."""
+    if not Path(path).exists():
+        return None
+    lines = Path(path).read_text().splitlines()
+    row = dict(zip(lines[0].split(","), lines[1].split(",")))
+    meta = json.loads(Path(path).with_suffix(".json").read_text())
+    return {"steps": [int(row[f"steps_{t}"]) for t in TAGS],
+            "q": np.array([[float(row[f"q{c}_{t}"]) for c in "xyz"] for t in TAGS]),
+            "K": np.array([[float(row[f"K_{a}{b}"]) for b in "xyz"] for a in "xyz"]),
+            "sha256": meta["sha256"], "seconds": meta["seconds"], "path": str(Path(path).relative_to(ROOT))}
 
 
 def log(*a):
@@ -157,27 +183,38 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(prec):
-    """DRAM bytes (read + write) per step launch of a path's step kernels, the
-    mean of one odd and one even launch, from the committed ncu summary."""
-    for p in sorted((ROOT / "profiles").glob("*_tensor128.md")):
-        m = re.search(r"traffic_bytes_per_launch\[" + re.escape(prec) + r"\]:\s*([0-9.eE+]+)", p.read_text())
-        if m:
-            return float(m.group(1))
-    return None
+TRAFFIC = ROOT / "profiles" / "traffic.json"
+
+
+def profiled_traffic(prec, variant, updates_per_launch):
+    """DRAM bytes (read + write) per step launch of this run's step kernels,
+    from the ncu capture recorded in profiles/traffic.json (per pore-voxel
+    update, the mean of one odd and one even launch, with the command that
+    measured it), scaled to this run's updates per launch.  None when no
+    capture of this precision and kernel variant is recorded."""
+    if not TRAFFIC.exists():
+        return None
+    rec = json.loads(TRAFFIC.read_text()).get(prec)
+    if not rec or rec.get("variant") != variant:
+        return None
+    return rec["dram_bytes_per_update"] * updates_per_launch
 
 
 def tensor_K(runs, mu, F):
     return np.array([[mu * runs[j].q[c] / F for j in range(3)] for c in range(3)])
 
 
-def k_errors(K, K64):
-    """Per-entry relative error of K against the FP64 K; off-diagonals are
-    judged against the trace scale (they are ~0 for this axis-aligned packing)."""
-    scale = np.abs(np.diag(K64)).max()
-    diag = float(max(abs(K[i, i] - K64[i, i]) / abs(K64[i, i]) for i in range(3)))
-    off = float(max(abs(K[i, j] - K64[i, j]) for i in range(3) for j in range(3) if i != j) / scale)
-    return {"max_rel_diag": diag, "max_offdiag_over_kmax": off, "max_rel": max(diag, off)}
+def k_errors(K, Kref):
+    """Per-entry error of K against Kref: |dK_ij| / |Kref_ij| on the diagonal,
+    / max_i |Kref_ii| off it (the off-diagonals of this axis-aligned packing
+    are differences of nearly cancelling sums, ~1e-3 of the diagonal)."""
+    scale = np.abs(np.diag(Kref)).max()
+    den = np.where(np.eye(3, dtype=bool), np.abs(Kref), scale)
+    m = np.abs(K - Kref) / den
+    diag = float(np.diag(m).max())
+    off = float(m[~np.eye(3, dtype=bool)].max())
+    return {"matrix": m.tolist(), "max_rel_diag": diag, "max_offdiag_over_kmax": off,
+            "max_rel": max(diag, off)}
 
 
 class EventTimer:
@@ -242,56 +279,96 @@ def cpu_sample(solid, wl, seconds_target=12.0, steps=None):
                        f"{cores} processes")
 
 
-def cpu_baseline_entry(cpu, N, steps64):
-    """k-tensors/hour of the CPU solver extrapolated with the FP64 step counts."""
-    lu_tensor = N * float(sum(steps64))
+def cpu_baseline_entry(cpu, N, steps, steps_source):
+    """k-tensors/hour of the CPU solver: its measured all-node rate on the
+    fixed-step sample, extrapolated to a converged tensor with `steps`."""
+    lu_tensor = N * float(sum(steps))
     sec_tensor = lu_tensor / cpu["lups_per_core"]
     return {"value": 3600.0 * cpu["cores"] / sec_tensor, "unit": "k-tensors/hr", "cores": cpu["cores"],
-            "kind": cpu["kind"], "sample": cpu["sample"] + "; extrapolated with FP64 step counts "
-            f"{list(map(int, steps64))}", "mlups_per_core": cpu["lups_per_core"] / 1e6}
+            "kind": cpu["kind"], "extrapolated": True,
+            "formula": "cores x 3600 / (N x sum(steps) / all-node LUPS per core)",
+            "steps_per_tensor": list(map(int, steps)), "steps_source": steps_source,
+            "sample": cpu["sample"], "sample_seconds": cpu["seconds"],
+            "mlups_per_core": cpu["lups_per_core"] / 1e6}
 
 
 # ---------------------------------------------------------------- serving ----
+def _serve_pool_entry(d):
+    from flow_anizotropy_b200 import structures as st
+    return st.make(d)
+
+
 def serve_trace(device, prec, args):
-    """Short Poisson trace at the serving rate (20 requests/s) through the
-    continuous-batching server: structures of the uneven-size mix restricted
-    to its two smallest edges (48, 64) so the trace drains in seconds."""
+    """The serving configuration: a Poisson stream at 20 requests/s for
+    --serve-seconds; every request is a structure of the uneven-size batch
+    mix (edges 48..160), and every 20th a 256^3 Gaussian-random-field sample
+    (phi in U[0.15, 0.35]), each asking for a 3-direction tensor at eps 1e-6
+    under a 150 GiB admission budget.  The requests draw from a pool of
+    seeded structures built before the trace (structure generation is not
+    timed).  At this rate the GPU is overloaded, so the trace runs for the
+    arrival window and stops: throughput is the requests completed in the
+    window, latencies are those of the completed requests, and the queue left
+    at the end is reported.  The plain FP32 rate is the same mix solved one
+    structure at a time."""
+    import multiprocessing as mproc
+    from flow_anizotropy_b200 import solver as S
     from flow_anizotropy_b200 import structures as st
     from flow_anizotropy_b200.serve import Server, poisson_arrivals, replay
-    from flow_anizotropy_b200.solver import Params3D
-    mix = [d for d in st.batch_mix(64, seed=5) if d["n"] in (48, 64)][:8]
-    pool = [st.make(d) for d in mix]
+    descs = [st.serving_request(i, seed=3) for i in range(args.serve_pool * 20 // 19 + 40)]
+    mix_d = [d for d in descs if d["kind"] != "grf"][:args.serve_pool]
+    grf_d = [d for d in descs if d["kind"] == "grf"][:2]
+    with mproc.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        built = pool.map(_serve_pool_entry, mix_d + grf_d)
+    mix, grf = built[:len(mix_d)], built[len(mix_d):]
     F = 2.5e-7 * WORKLOAD["ff"]
-    p = Params3D(tau=1.0, eps=WORKLOAD["eps"], lag=WORKLOAD["lag"], hold=WORKLOAD["hold"],
-                 min_steps=WORKLOAD["min_steps"], max_steps=WORKLOAD["max_steps"],
-                 avg_steps=WORKLOAD["avg_steps"], precision=prec)
+    p = S.Params3D(tau=1.0, eps=WORKLOAD["eps"], lag=WORKLOAD["lag"], hold=WORKLOAD["hold"],
+                   min_steps=WORKLOAD["min_steps"], max_steps=WORKLOAD["max_steps"],
+                   avg_steps=WORKLOAD["avg_steps"], precision=prec)
     forces = [[F, 0, 0], [0, F, 0], [0, 0, F]]
+
+    def request(i):
+        if i % 20 == 19:
+            return grf[(i // 20) % len(grf)], forces, p
+        return mix[(i - i // 20) % len(mix)], forces, p
+
     srv = Server(precision=prec, hbm_budget=150 * 2**30, chunk=128, device=device, variant=args.serve_variant)
     arrivals = poisson_arrivals(20.0, args.serve_seconds, seed=11)
     t0 = time.perf_counter()
-    stats = replay(srv, arrivals, lambda i: (pool[i % len(pool)], forces, p))
+    stats = replay(srv, arrivals, request, horizon=args.serve_seconds)
     wall = time.perf_counter() - t0
+    queued, resident = len(srv.queue), len(srv.inflight)
     srv.close()
     served = stats.completed / wall
-    # plain FP32 on the same structures, one tensor at a time, each with the
-    # step-kernel variant the autotuner picks for it (tuning not timed): the
-    # baseline the served throughput is compared with
-    from flow_anizotropy_b200 import solver as S
-    tuned = [S.tune3d(s_, ndir=3, precision="fp32", nsteps=100, device=device)[0] for s_ in pool]
-    pps = [Params3D(**{**p.__dict__, "precision": "fp32", "variant": v}) for v in tuned]
-    S.solve3d(pool[0], forces, pps[0], device=device)
+    # plain FP32, one structure at a time with the library's default FP32
+    # kernels, on a sample of the same mix weighted as the stream is (19 mix
+    # requests to 1 GRF)
+    pp = S.Params3D(**{**p.__dict__, "precision": "fp32"})
+    nplain = min(len(mix), args.serve_plain_sample)
+    S.solve3d(mix[0], forces, pp, device=device)
     t0 = time.perf_counter()
-    for s_, pp in zip(pool, pps):
+    for s_ in mix[:nplain]:
         S.solve3d(s_, forces, pp, device=device)
-    plain = len(pool) / (time.perf_counter() - t0)
-    return {"rate_per_s": 20.0, "arrival_seconds": args.serve_seconds, "requests": stats.completed,
-            "p50_s": stats.pct(50), "p99_s": stats.pct(99), "max_resident": stats.max_resident,
+    t_mix = (time.perf_counter() - t0) / nplain
+    t0 = time.perf_counter()
+    S.solve3d(grf[0], forces, pp, device=device)
+    t_grf = time.perf_counter() - t0
+    plain = 1.0 / (0.95 * t_mix + 0.05 * t_grf)
+    lat = np.array(stats.latencies) if stats.latencies else np.array([np.nan])
+    return {"rate_per_s": 20.0, "arrival_seconds": args.serve_seconds, "arrived": len(arrivals),
+            "completed": stats.completed, "left_queued": queued, "left_resident": resident,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "p50_queue_s": float(np.percentile(stats.queue_waits, 50)) if stats.queue_waits else None,
             "k_tensors_per_hr": 3600.0 * served, "served_per_s": served, "overloaded": 20.0 > served,
-            "plain_fp32_per_s": plain, "speedup_vs_plain_fp32": served / plain,
+            "max_resident": stats.max_resident, "max_resident_gib": stats.max_resident_bytes / 2**30,
+            "plain_fp32_per_s": plain,
+            "plain_fp32_sample": f"{nplain} mix structures + 1 GRF, weighted 19:1",
+            "speedup_vs_plain_fp32": served / plain,
             "admission": f"FIFO, HBM budget 150 GiB, resident work cap {srv.max_work} pore-voxel-directions",
-            "mix": "batch mix, edges 48 and 64 only (8 seeded structures, reused)", "path": prec,
-            "batch_variant": args.serve_variant}
+            "mix": f"pool of {len(mix)} batch-mix structures (edges {sorted(set(d['n'] for d in mix_d))}) "
+                   f"and {len(grf)} 256^3 GRF samples (every 20th request)",
+            "path": prec, "batch_variant": args.serve_variant,
+            "latency_note": "latencies of the requests completed within the window (an overloaded "
+                            "server's queue grows without bound, so they understate the steady state)"}
 
 
 # -------------------------------------------------------------- our arm ----
@@ -313,18 +390,25 @@ def run_ours(args, rank, world, local_rank):
     solid = st.ellipsoid_packing(wl["n"], wl["semi"], wl["porosity"], wl["seed"])
     N = solid.size
     npore = int((solid == 0).sum())
+    phi = npore / N
     F = 2.5e-7 * wl["ff"]
     forces = [[F, 0, 0], [0, F, 0], [0, 0, F]]
     mu = (1.0 / 3.0) * (wl["tau"] - 0.5)
     ctx = _lib.context(device)
     solid_dev = torch.from_numpy(np.ascontiguousarray(solid)).cuda(device)
+    ref = reference_row()
+    if ref is not None:
+        import hashlib
+        if hashlib.sha256(np.ascontiguousarray(solid).tobytes()).hexdigest() != ref["sha256"]:
+            log("reference row was written for another structure: not used")
+            ref = None
 
     def params(prec, variant=0):
         return S.Params3D(tau=wl["tau"], eps=wl["eps"], lag=wl["lag"], hold=wl["hold"], min_steps=wl["min_steps"],
                           max_steps=wl["max_steps"], avg_steps=wl["avg_steps"], precision=prec,
                           criterion="auto", variant=variant)
 
-    # FP64 oracle solve on the GPU (the reference's arithmetic), untimed
+    # FP64 solve on the GPU (the reference's arithmetic), untimed
     r64, _, _ = S.solve3d(solid_dev, forces, params("fp64"), device=device)
     K64 = tensor_K(r64, mu, F)
     steps64 = [r.steps for r in r64]
@@ -357,13 +441,14 @@ def run_ours(args, rank, world, local_rank):
                     dir_steps=dir_steps, launches=launches)
 
     results = {}
-    cands = [args.precision] if args.precision != "auto" else ["fp32", "fp16", "m32", "md32"]
+    cands = [args.precision] if args.precision != "auto" else ["fp32", "fp16", "bf16"]
     if "fp32" not in cands:
         cands.append("fp32")
     for prec in cands:
         m = measure(prec, args.warmup, args.steps)
         m["K"] = tensor_K(m["runs"], mu, F)
         m["err"] = k_errors(m["K"], K64)
+        m["err_ref"] = k_errors(m["K"], ref["K"]) if ref is not None else None
         results[prec] = m
 
     def rates(m):
@@ -384,21 +469,30 @@ def run_ours(args, rank, world, local_rank):
     alg_bytes = head["dir_steps"] * alg_bytes_per_dir_step(head_prec, npore, N)
     achieved = alg_bytes / (head["ms"] / 1e3) / 1e9
     per_launch_alg = alg_bytes / max(1, head["launches"])
-    traffic = profiled_traffic(head_prec)
-    serving = serve_trace(device, args.serve_precision, args) if args.serve_seconds > 0 else None
+    updates_per_launch = head["dir_steps"] * npore / max(1, head["launches"])
+    traffic = profiled_traffic(head_prec, head["variant"], updates_per_launch)
+    legs = world == 1
+    serving = serve_trace(device, args.serve_precision, args) if legs and args.serve_seconds > 0 else None
+    large = run_large_workload(args, device) if legs and args.large_steps > 0 else None
+    batch = run_batch_workload(args, device) if legs and args.count > 0 else None
     out = None
     if rank == 0:
         cpu = cpu_sample(solid, wl, seconds_target=args.cpu_seconds)
-        cpu_entry = cpu_baseline_entry(cpu, N, steps64)
+        if ref is not None:
+            cpu_entry = cpu_baseline_entry(cpu, N, ref["steps"], f"the reference's own run ({ref['path']})")
+        else:
+            cpu_entry = cpu_baseline_entry(cpu, N, steps64, "the GPU FP64 solve (no reference row present)")
         paths = {}
         for p_, m in results.items():
             k_, g_, a_ = rates(m)
             paths[p_] = {"k_tensors_per_hr": k_, "glups_fluid": g_, "glups_all_node": a_,
                          "steps_per_direction": [r.steps for r in m["runs"]],
                          "converged": [r.converged for r in m["runs"]],
-                         "rel_err_vs_fp64": m["err"], "kernel_variant": m["variant"],
+                         "rel_err_vs_fp64": m["err"], "rel_err_vs_reference": m["err_ref"],
+                         "kernel_variant": m["variant"],
                          "hbm_gbs_alg": m["dir_steps"] * alg_bytes_per_dir_step(p_, npore, N) / (m["ms"] / 1e3) / 1e9,
                          "clocks": m["clocks"]}
+        qh = np.array([r.q for r in head["runs"]])
         out = {
             "metric": METRIC, "value": kt, "unit": "k-tensors/hr", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
@@ -408,24 +502,29 @@ def run_ours(args, rank, world, local_rank):
                        "eps": wl["eps"], "lag": wl["lag"], "hold": wl["hold"], "min_steps": wl["min_steps"],
                        "max_steps": wl["max_steps"], "avg_steps": wl["avg_steps"],
                        "path": head_prec, "kernel_variant": head["variant"],
-                       "criterion": "block means, batch-means SE, k-sigma" if head_prec in ("fp16", "bf16") else "drift (reference)",
+                       "criterion": "block means, batch-means SE, k-sigma" if head_prec in ("fp16", "bf16")
+                       else "drift (reference)",
                        "parallelism": f"work partition x{world} (one tensor stream per GPU)",
                        "l2": "lattices (3 x 19 x 0.94 M pores x elem: 215 MB fp32, 108 MB fp16) stream from HBM "
                              "every step; inputs are the whole tensor solve, not a cached kernel"},
             "glups_fluid": gf, "glups_all_node": ga,
             "steps_per_direction": [r.steps for r in head["runs"]],
-            "rel_err_vs_fp64": head["err"],
+            "rel_err_vs_fp64": head["err"], "rel_err_vs_reference": head["err_ref"],
+            "mean_velocity": {"superficial_q": qh.tolist(), "pore_mean_q_over_phi": (qh / phi).tolist(),
+                              "porosity": phi, "rows": "forcing direction x, y, z; columns q_x, q_y, q_z"},
             "paths": paths,
             "plain_fp32": {"value": kt_p, "unit": "k-tensors/hr", "glups_fluid": gf_p, "glups_all_node": ga_p},
             "speedup_vs_plain_fp32": kt / kt_p,
             "fp64_steps_per_direction": steps64,
-            "serving": serving,
+            "reference_steps_per_direction": ref["steps"] if ref is not None else None,
+            "serving": serving, "large": large, "batch": batch,
             "e2e": {"value": kt_e, "unit": "k-tensors/hr", "h2d_bytes_per_step": int(N),
                     "d2h_bytes_per_step": int(3 * 64)},
-            "gpu_launches": int(head["launches"] + 8 * args.steps),
+            "gpu_launches": int(head["launches"] + head["launches"] // 64 + 9 * args.steps),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "alg_bytes_per_launch": per_launch_alg,
+                         "traffic_source": str(TRAFFIC.relative_to(ROOT)) if traffic is not None else None,
                          "kernel": f"step3d ({head_prec}) variant {head['variant']}"},
             "cpu_baseline": cpu_entry,
             "clocks": head["clocks"],
@@ -443,10 +542,12 @@ def _make_structure(d):
 
 
 def run_batch_workload(args, device=0):
-    """The uneven-size mix: `count` structures with edges from {48,64,96,128,160},
-    three directions each, solved (a) one structure at a time with plain FP32
-    per-step launches, (b) all resident in one batch (CUDA-graph chunks,
-    per-solve retirement) for each batched path.  Reports k-tensors/hour."""
+    """The uneven-size mix: the first `count` structures of the seeded
+    256-structure mix (edges from {48,64,96,128,160}; the generator draws
+    them in order, so they are the same structures), three directions each,
+    solved (a) one structure at a time with plain FP32 per-step launches, (b)
+    all resident in one batch (CUDA-graph chunks, per-solve retirement) for
+    each batched path.  Reports k-tensors/hour."""
     import multiprocessing as mproc
     import torch
     from flow_anizotropy_b200 import _lib
@@ -464,7 +565,8 @@ def run_batch_workload(args, device=0):
                           min_steps=WORKLOAD["min_steps"], max_steps=WORKLOAD["max_steps"],
                           avg_steps=WORKLOAD["avg_steps"], precision=prec)
 
-    out = {"workload": f"batch mix of {args.count} structures (edges 48..160, 3 directions)",
+    out = {"workload": f"first {args.count} structures of the 256-structure batch mix (edges 48..160, "
+                       f"3 directions each)",
            "voxels": int(sum(s.size for s in structs)), "pores": int(sum((s == 0).sum() for s in structs))}
     ref = {}
     with EventTimer(torch, ctx.stream) as t:
@@ -627,30 +729,77 @@ def run_perm2d_workload(args, device=0):
     return out
 
 
+# ------------------------------------------------------ fixed-step runs ----
+STEP_STRUCTURES = {"tensor128": "precision_128", "plain64": "plain_64"}
+
+
+def run_steps_workload(args, device=0):
+    """A fixed number of steps of one precision and kernel variant on a named
+    structure, all three forcing directions together (no convergence stop, no
+    averaging): the command the kernel profiles in profiles/ capture.  With
+    --images N it runs N 256^2 D2Q9 disc packings, both directions, instead."""
+    from flow_anizotropy_b200 import solver as S
+    from flow_anizotropy_b200 import structures as st
+    if args.images > 0:
+        imgs = np.stack([st.disc_packing_2d(seed=i, solid_fraction=0.2 + 0.05 * (i % 5)) for i in range(args.images)])
+        p2 = S.Params2D(tau=args.tau, lag=args.steps + 1, min_steps=args.steps + 1, max_steps=args.steps, avg_steps=0)
+        runs, _ = S.solve2d_many(imgs, [[S.FX_BASE, 0.0], [0.0, S.FX_BASE]], p2, device=device)
+        return {"workload": f"D2Q9 {args.images} images x 2 directions, {args.steps} steps",
+                "steps": [[r.steps for r in rr] for rr in runs[:2]]}
+    solid = getattr(st, STEP_STRUCTURES[args.structure])(0)
+    prec = "fp32" if args.precision == "auto" else args.precision
+    variant = args.variant
+    if variant < 0:
+        variant, _ = S.tune3d(solid, ndir=3, precision=prec, nsteps=50, device=device)
+    F = 1e-6
+    p = S.Params3D(precision=prec, criterion="drift", tau=args.tau, lag=args.lag, max_steps=args.steps,
+                   avg_steps=0, hold=10**6, variant=variant)
+    runs, _, _ = S.solve3d(solid, [[F, 0, 0], [0, F, 0], [0, 0, F]], p, device=device)
+    return {"workload": f"{args.structure} fixed steps", "precision": prec, "variant": variant,
+            "steps": [r.steps for r in runs], "q": [list(map(float, r.q)) for r in runs]}
+
+
 # -------------------------------------------------------- reference arm ----
 def run_reference(args, rank, world):
+    """The reference CPU solver (oracle/_ref/lbm3d-perm, built from
+    LMB3d/lbm3d-perm.cpp with its own flags) on all host cores, one process
+    per core as scripts/solve_permeability3d.py runs it.  Each bench step is
+    one bounded fixed-step sample of the workload structure (every process
+    solves the three directions for a few steps); `steps` and `ms_per_step`
+    are those samples as timed.  `value` turns the measured all-node rate into
+    converged k-tensors/hour with the step counts the reference itself took
+    on this structure (tests/golden/configs/precision128.csv; a full
+    converged tensor takes the reference about an hour per core), and says so
+    in `extrapolated`."""
     if rank != 0:
         return None
     from flow_anizotropy_b200 import structures as st
     wl = dict(WORKLOAD)
+    ref = reference_row()
+    if ref is None:
+        return {"impl": "reference", "unavailable": f"no reference row at {REF_ROW.relative_to(ROOT)}"}
     solid = st.ellipsoid_packing(wl["n"], wl["semi"], wl["porosity"], wl["seed"])
     N = solid.size
-    steps64 = FP64_STEPS
-    per_step = []
-    cpu = None
+    samples = []
     for i in range(args.warmup + args.steps):
         cpu = cpu_sample(solid, wl, seconds_target=args.cpu_seconds)
         if i >= args.warmup:
-            per_step.append(cpu)
-    lups = statistics.median(c["lups_per_core"] for c in per_step)
-    cpu = dict(per_step[-1], lups_per_core=lups)
-    entry = cpu_baseline_entry(cpu, N, steps64)
+            samples.append(cpu)
+    lups = statistics.median(c["lups_per_core"] for c in samples)
+    cpu = dict(samples[-1], lups_per_core=lups)
+    entry = cpu_baseline_entry(cpu, N, ref["steps"], f"the reference's own run ({ref['path']})")
+    sample_ms = 1e3 * statistics.mean(c["seconds"] for c in samples)
     return {"metric": METRIC, "value": entry["value"], "unit": "k-tensors/hr", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * float(sum(steps64)) * N / (lups * cpu["cores"]), "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded structure)",
-            "config": {"workload": wl["workload"], "seed": wl["seed"], "precision": "fp64"},
-            "impl": "reference", "cpu_baseline": entry,
+            "config": {"workload": wl["workload"], "seed": wl["seed"], "precision": "fp64",
+                       "step": "one fixed-step sample on all host cores (" + cpu["sample"] + ")"},
+            "impl": "reference",
+            "extrapolated": {"value_from": "median all-node LUPS per core of the timed samples",
+                             "formula": entry["formula"], "steps_per_tensor": ref["steps"],
+                             "steps_source": entry["steps_source"],
+                             "converged_tensor_seconds_per_core": N * float(sum(ref["steps"])) / lups},
+            "cpu_baseline": entry,
             "e2e": {"value": entry["value"], "unit": "k-tensors/hr", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -662,18 +811,30 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32", "md32"])
-    ap.add_argument("--serve-seconds", type=float, default=5.0)
+    ap.add_argument("--serve-seconds", type=float, default=120.0,
+                    help="arrival window of the serving leg (0: no serving leg)")
     ap.add_argument("--serve-precision", default="fp16", choices=["fp32", "fp16", "bf16"])
-    ap.add_argument("--serve-variant", type=int, default=1,
-                    help="step-kernel variant of the serving batch (-1: library default; 1 measured "
-                         "fastest for FP16 on the 48^3-64^3 serving mix)")
-    ap.add_argument("--workload", default="tensor128", choices=["tensor128", "batch", "gen3d", "large", "perm2d"])
+    ap.add_argument("--serve-variant", type=int, default=-1,
+                    help="step-kernel variant of the serving batch (-1: library default)")
+    ap.add_argument("--serve-pool", type=int, default=40, help="distinct batch-mix structures the requests draw")
+    ap.add_argument("--serve-plain-sample", type=int, default=10,
+                    help="structures of the plain FP32 one-at-a-time comparison")
+    ap.add_argument("--workload", default="tensor128",
+                    choices=["tensor128", "batch", "gen3d", "large", "perm2d", "steps"])
+    ap.add_argument("--structure", default="tensor128", choices=sorted(STEP_STRUCTURES),
+                    help="structure of the steps workload")
+    ap.add_argument("--variant", type=int, default=-1, help="steps workload: step-kernel variant (-1: autotune)")
+    ap.add_argument("--tau", type=float, default=1.0, help="steps workload: relaxation time")
+    ap.add_argument("--lag", type=int, default=10**9,
+                    help="steps workload: reduce the flux every LAG steps (1: every step, as in the averaging phase)")
+    ap.add_argument("--images", type=int, default=0, help="steps workload: D2Q9 images instead of a 3D structure")
     ap.add_argument("--group2d", type=int, default=16, help="images per launch of the perm2d workload")
     ap.add_argument("--large-n", type=int, default=512, help="cell edge of the large workload")
-    ap.add_argument("--large-steps", type=int, default=2000)
+    ap.add_argument("--large-steps", type=int, default=2000, help="fixed steps of the large leg (0: no large leg)")
     ap.add_argument("--gen-size", type=int, default=80, help="cell edge of the gen3d workload")
-    ap.add_argument("--count", type=int, default=32, help="structures of the batch workload")
-    ap.add_argument("--batch-paths", default="fp32,m32,fp16")
+    ap.add_argument("--count", type=int, default=48,
+                    help="structures of the batch leg / workload (0: no batch leg)")
+    ap.add_argument("--batch-paths", default="fp16")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -689,6 +850,8 @@ def main():
         out = run_large_workload(args, local_rank) if rank == 0 else None
     elif args.workload == "perm2d":
         out = run_perm2d_workload(args, local_rank) if rank == 0 else None
+    elif args.workload == "steps":
+        out = run_steps_workload(args, local_rank) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None and rank == 0:

@@ -1,6 +1,6 @@
 """Host-side pieces of bench.py (no GPU): the roofline byte model, the
-traffic figures read from the committed ncu summaries, the clock-sample
-summary, and the command line."""
+traffic figure scaled from the recorded ncu capture, the reference row, the
+per-k_ij error matrix, the clock-sample summary, and the command line."""
 import subprocess
 import sys
 from pathlib import Path
@@ -20,20 +20,35 @@ def test_algorithmic_bytes_model():
     assert bench.alg_bytes_per_dir_step("md32", npore, nvox) == 21.0 * nvox + 20.0 * npore
 
 
-def test_profiled_traffic_read_from_profiles():
-    for prec in ("fp32", "fp16", "md32"):
-        v = bench.profiled_traffic(prec)
-        assert v is not None and 1e8 < v < 1e9, (prec, v)
-        alg = 3 * bench.alg_bytes_per_dir_step(prec, 943_600, 128 ** 3)
-        if prec != "md32":
-            # the population kernels move no more DRAM bytes per launch than
-            # the algorithmic bytes of three directions: no wasted re-reads
-            assert v <= alg, (prec, v, alg)
-        else:
-            # the dense moment form re-reads the halo rows L2 does not keep
-            # (its summary says so): within 2x of its algorithmic bytes
-            assert v <= 2 * alg, (prec, v, alg)
-    assert bench.profiled_traffic("no-such-path") is None
+def test_profiled_traffic_scaled_from_the_recorded_capture(tmp_path, monkeypatch):
+    rec = {"fp16": {"variant": 7, "dram_bytes_per_update": 70.0, "command": "ncu ..."}}
+    f = tmp_path / "traffic.json"
+    f.write_text(__import__("json").dumps(rec))
+    monkeypatch.setattr(bench, "TRAFFIC", f)
+    assert bench.profiled_traffic("fp16", 7, 1000.0) == 70_000.0
+    assert bench.profiled_traffic("fp16", 8, 1000.0) is None        # another kernel variant: not this capture
+    assert bench.profiled_traffic("fp32", 7, 1000.0) is None
+    monkeypatch.setattr(bench, "TRAFFIC", tmp_path / "absent.json")
+    assert bench.profiled_traffic("fp16", 7, 1000.0) is None
+
+
+def test_recorded_traffic_within_the_algorithmic_bytes():
+    """The recorded captures move no more DRAM bytes per update than the
+    algorithmic ones (populations read and written once): no wasted re-reads."""
+    import json
+    if not bench.TRAFFIC.exists():
+        return
+    for prec, rec in json.loads(bench.TRAFFIC.read_text()).items():
+        alg = bench.BYTES_PER_UPDATE[prec] + 1.0 / 8 / 0.45
+        assert 0 < rec["dram_bytes_per_update"] <= 1.05 * alg, (prec, rec)
+
+
+def test_reference_row_of_the_workload():
+    ref = bench.reference_row()
+    if ref is None:
+        return
+    assert len(ref["steps"]) == 3 and all(s > 0 for s in ref["steps"])
+    assert ref["K"].shape == (3, 3) and (np.diag(ref["K"]) > 0).all()
 
 
 def test_clock_summary(tmp_path):
@@ -58,6 +73,9 @@ def test_k_errors_relative_to_fp64():
     e = bench.k_errors(K, K64)
     assert abs(e["max_rel_diag"] - 1e-6) < 1e-12
     assert abs(e["max_offdiag_over_kmax"] - 1e-8) < 1e-14
+    m = np.array(e["matrix"])
+    assert m.shape == (3, 3) and abs(m[0, 0] - 1e-6) < 1e-12 and abs(m[0, 1] - 1e-8) < 1e-14
+    assert m[1, 1] == 0 and m[2, 0] == 0
 
 
 def test_command_line():
@@ -65,5 +83,5 @@ def test_command_line():
                          timeout=300)
     assert out.returncode == 0
     for flag in ("--gpus", "--steps", "--warmup", "--impl", "--workload", "--serve-precision", "--serve-variant",
-                 "--group2d"):
+                 "--group2d", "--serve-seconds", "--large-steps", "--count", "--variant", "--structure"):
         assert flag in out.stdout, flag
