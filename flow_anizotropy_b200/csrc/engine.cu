@@ -172,12 +172,21 @@ int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
 }
 
 // The autotuner's pick on the 128^3 tensor workload: FP32 plain odd + even
-// ranks from the mask; 16-bit bulk-staged odd + even from neighbour records.
+// ranks from the mask; 16-bit bulk-staged odd + grouped even step with the
+// link slots shared by the directions and voxel pairs collided together.
 int lbm_default_variant(int prec)
 {
     if (prec == LBM_FP32) return 0 * NVAR_EVEN_LP + 3;
-    if (prec == LBM_FP16 || prec == LBM_BF16) return 4 * NVAR_EVEN_LP + 1;
+    if (prec == LBM_FP16 || prec == LBM_BF16) return 4 * NVAR_EVEN_LP + 11;
     return 0;
+}
+
+// The batch steps each direction on its own (no grouped even kernels): its
+// default is the best per-direction pick, even step from neighbour records.
+int lbm_default_batch_variant(int prec)
+{
+    if (prec == LBM_FP16 || prec == LBM_BF16) return 4 * NVAR_EVEN_LP + 1;
+    return lbm_default_variant(prec);
 }
 
 static lbm_params3d lbm_resolve_variant(lbm_params3d p)
@@ -215,6 +224,7 @@ int lbm_effective_variant(int prec, int variant, bool have_meta)
     if (is_moment(prec) || is_dense_m(prec) || have_meta) return variant;
     const int ve = variant % nvar_even(prec);
     if (!even_meta(ve)) return variant;
+    if (even_wide(ve)) return variant - ve + 14;        // link slots, one voxel per thread, ranks from the mask
     if (even_links(ve)) return variant - ve + 10;       // grouped link slots (one voxel at a time), ranks from the mask
     if (even_grouped(ve)) return variant - ve + 6;      // grouped, ranks from the mask
     return variant - ve + (ve & 1) + 2;                 // same budget, ranks from the mask
@@ -453,7 +463,7 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
     // before a chunk reuses their slots, and before the states are read)
     auto flush = [&]() -> cudaError_t {
         if (!pending) return cudaSuccess;
-        const cudaError_t e = launch_deferred3d(d_solves, n, pend0, pending, qb, ctx->stream);
+        const cudaError_t e = launch_deferred3d(d_solves, n, pend0, pending, qb, 1, ctx->stream);
         pending = 0;
         return e;
     };
@@ -478,7 +488,7 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
             cudaError_t e = cudaSuccess;
             // launch i of a chunk runs step i + 1 after s_base (s_base even)
             for (int i = 0; i < kGraphSteps3 && e == cudaSuccess; ++i) e = launch(i, ((i + 1) & 1) == 1);
-            if (e == cudaSuccess && defer) e = launch_deferred3d(d_solves, n, 0, kGraphSteps3, qb, ctx->stream);
+            if (e == cudaSuccess && defer) e = launch_deferred3d(d_solves, n, 0, kGraphSteps3, qb, 1, ctx->stream);
             if (e == cudaSuccess) {
                 advance3d_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(d_solves, n, kGraphSteps3);
                 e = cudaGetLastError();

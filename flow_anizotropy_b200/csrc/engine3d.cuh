@@ -316,6 +316,28 @@ __device__ __forceinline__ int defer_slot(const StepArgs &a)
     return a.defer ? (int)(a.step & (DEFER_SLOTS - 1)) : -1;
 }
 
+// Does a deferred step write (and the reduction pass sum) its flux partials?
+// The steps the controller needs at the phase of the run (`pass_start`:
+// steps done before the current reduction pass), and, with mode 2 (runs in
+// which a solve's phase can change between passes, as in a batch whose
+// solves sit at different step counts), every step after a lag multiple or
+// max_steps since the pass started: the controller may have left phase 1
+// there and then needs every step.
+__device__ __forceinline__ bool deferred_reduces(const Ctl3 &c, int phase, long long n, long long pass_start, int mode)
+{
+    if (needs_reduction(c, phase, n)) return true;
+    if (mode != 2 || phase != PH_RUN) return false;
+    return (n - 1) / c.lag > pass_start / c.lag || (c.max_steps > pass_start && c.max_steps < n);
+}
+
+// Reduction flag of step n (= s_base + a.step + 1) of a solve in a launch.
+__device__ __forceinline__ bool step_reduces(const StepArgs &a, const Ctl3 &c, int phase, long long n)
+{
+    if (a.defer != 2) return needs_reduction(c, phase, n);
+    const long long s_base = n - a.step - 1;
+    return deferred_reduces(c, phase, n, s_base + (a.step & ~(long long)(DEFER_SLOTS - 1)), 2);
+}
+
 // Tile finished on a reduction step: publish the tile's flux partial; the
 // last tile of the solve to finish sums all partials in a fixed order (the
 // result does not depend on which blocks ran which tiles, or on what else is
@@ -493,7 +515,7 @@ __device__ __forceinline__ void meta_nbrs(const Solve3 &S, unsigned i, const uin
 // (NVAR_EVEN_LP for the reduced-precision storage, which adds the grouped
 // even kernels); lbm_tune3d times them on the actual structure.
 struct Variant { int npt, minb; };
-constexpr int NVAR_ODD = 3, NVAR_ODD_LP = 5, NVAR_EVEN = 6, NVAR_EVEN_LP = 13;
+constexpr int NVAR_ODD = 3, NVAR_ODD_LP = 5, NVAR_EVEN = 6, NVAR_EVEN_LP = 15;
 constexpr int NVAR_LP = NVAR_ODD_LP * NVAR_EVEN_LP, NVAR_F64 = NVAR_ODD * NVAR_EVEN;
 constexpr int MAX_GROUP = 3;    // directions per grouped even step
 inline int nvar_even(int prec) { return prec == 0 ? NVAR_EVEN : NVAR_EVEN_LP; }
@@ -510,19 +532,24 @@ __host__ __device__ constexpr Variant odd_lp(int v)
 // from the mask, 7 from the record), 8-12 are grouped with the link slots
 // kept in shared memory and the directions stepped one at a time (8-9 from
 // the record, 10 from the mask, 11-12 from the record with a thread's two
-// voxels collided together in packed FP32)
+// voxels collided together in packed FP32, 13-14 one voxel per thread in
+// blocks of 2 * TPB threads, 13 from the record, 14 from the mask)
 __host__ __device__ constexpr Variant even_lp(int v)
 {
     return v == 0 ? Variant{1, 3} : v == 1 ? Variant{1, 4} : v == 2 ? Variant{1, 3} : v == 3 ? Variant{1, 4}
          : v == 4 ? Variant{1, 4} : v == 5 ? Variant{1, 3} : v <= 7 ? Variant{1, 2}
          : v == 8 ? Variant{1, 3} : v == 9 ? Variant{1, 4} : v == 10 ? Variant{1, 3}
-         : v == 11 ? Variant{2, 3} : Variant{2, 2};
+         : v == 11 ? Variant{2, 3} : v == 12 ? Variant{2, 2} : Variant{1, 2};
 }
-__host__ __device__ constexpr bool even_meta(int v) { return v < 2 || v == 4 || v == 5 || v == 7 || v == 8 || v == 9 || v >= 11; }
+__host__ __device__ constexpr bool even_meta(int v)
+{
+    return v < 2 || v == 4 || v == 5 || v == 7 || v == 8 || v == 9 || v == 11 || v == 12 || v == 13;
+}
 __host__ __device__ constexpr bool even_async(int v) { return v == 4 || v == 5; }
 __host__ __device__ constexpr bool even_grouped(int v) { return v >= 6; }
 __host__ __device__ constexpr bool even_links(int v) { return v >= 8; }
-__host__ __device__ constexpr bool even_pair(int v) { return v >= 11; }
+__host__ __device__ constexpr bool even_pair(int v) { return v == 11 || v == 12; }
+__host__ __device__ constexpr bool even_wide(int v) { return v >= 13; }   // blocks of 2 * TPB threads
 __host__ __device__ constexpr Variant odd_f64(int v) { return v == 0 ? Variant{1, 2} : v == 1 ? Variant{2, 1} : Variant{1, 1}; }
 __host__ __device__ constexpr Variant even_f64(int v)
 {
@@ -601,7 +628,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
         const int phase = S.st->phase;
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
-        const bool red = needs_reduction(S.c, phase, n);
+        const bool red = step_reduces(a, S.c, phase, n);
         T *__restrict__ A = static_cast<T *>(S.A);
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
@@ -700,7 +727,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepAr
         const int phase = S.st->phase;
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
-        const bool red = needs_reduction(S.c, phase, n);
+        const bool red = step_reduces(a, S.c, phase, n);
         T *__restrict__ A = static_cast<T *>(S.A);
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
@@ -791,70 +818,106 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
 
     if (tid >= TPB) {
         // ------------------------------------------------------ producer --
-        if (tid != TPB || a.starve) return;
+        // lane 0 walks the work list, waits for free buffers and fills the
+        // tile descriptors; lanes 0..18 then issue one plane run each
+        if (a.starve) return;
+        const unsigned lane = (unsigned)tid & 31u;
         int next = blockIdx.x;
         unsigned eparity = 0u, fparity = 0u, copies = 0u;   // copies: buffers with bytes issued
+        // the fields of the last solve seen (items of one solve come in runs;
+        // nothing a tile needs changes during a launch once the solve is seen)
+        int cx = -1, cphase = PH_DONE, cred = 0;
+        BulkTile c{};
+        bool gave_up = false;
         for (int t = 0;; ++t) {
             const int s = t % NS;
-            if (t >= NS) {
-                // the consumers' release of this buffer's previous tile
-                if (!mbar_wait_bounded(&empty[s], (eparity >> s) & 1u, wait_ns)) break;
-                eparity ^= 1u << s;
-                copies &= ~(1u << s);
-            }
-            int w = next;
+            bool more = false;
             unsigned bytes = 0u, P = 0u;
             const T *src = nullptr;
-            BulkTile &d = slot[s];
-            for (; w < nwork; w += gridDim.x) {
-                const int2 it = a.work[w];
-                const Solve3 &S = a.solves[it.x];
-                const int phase = S.st->phase;
-                if (phase >= PH_DONE) continue;
-                const unsigned i0 = (unsigned)it.y * TV;
-                src = static_cast<const T *>(S.A) + i0;
-                P = (unsigned)S.plane;
-                if ((reinterpret_cast<uintptr_t>(src) | (uintptr_t)P * sizeof(T)) & 15u) {
-                    // not a legal bulk copy (lattices are allocated aligned
-                    // and planes padded to 64 slots, so this does not happen):
-                    // the solve is failed instead of copied
-                    S.st->status = STATUS_WAIT_TIMEOUT;
-                    S.st->phase = PH_ERR;
-                    continue;
+            if (lane == 0) {
+                if (t >= NS) {
+                    // the consumers' release of this buffer's previous tile
+                    if (!mbar_wait_bounded(&empty[s], (eparity >> s) & 1u, wait_ns)) {
+                        gave_up = true;
+                    } else {
+                        eparity ^= 1u << s;
+                        copies &= ~(1u << s);
+                    }
                 }
-                bytes = ((unsigned)min(TV, (unsigned)S.nfluid - i0) * (unsigned)sizeof(T) + 15u) & ~15u;
-                const long long n = S.st->s_base + a.step + 1;
-                d.A = S.A;
-                d.n = n;
-                d.tile_start = i0;
-                d.solve = it.x;
-                d.red = needs_reduction(S.c, phase, n) ? 1 : 0;
-                d.P = P;
-                d.nfluid = (unsigned)S.nfluid;
-                d.scale = S.scale;
-                d.inv_scale = S.inv_scale;
-                d.phys = S.P;
-                break;
+                if (!gave_up) {
+                    int w = next;
+                    BulkTile &d = slot[s];
+                    for (; w < nwork; w += gridDim.x) {
+                        const int2 it = a.work[w];
+                        if (it.x != cx) {
+                            const Solve3 &S = a.solves[it.x];
+                            cx = it.x;
+                            cphase = S.st->phase;
+                            c.A = S.A;
+                            c.n = S.st->s_base + a.step + 1;
+                            c.P = (unsigned)S.plane;
+                            c.nfluid = (unsigned)S.nfluid;
+                            c.scale = S.scale;
+                            c.inv_scale = S.inv_scale;
+                            c.phys = S.P;
+                            cred = cphase < PH_DONE && step_reduces(a, S.c, cphase, c.n) ? 1 : 0;
+                            if (cphase < PH_DONE && ((reinterpret_cast<uintptr_t>(S.A) | (uintptr_t)c.P * sizeof(T)) & 15u)) {
+                                // not a legal bulk copy (lattices are allocated
+                                // aligned and planes padded to 64 slots, so this
+                                // does not happen): the solve is failed instead
+                                S.st->status = STATUS_WAIT_TIMEOUT;
+                                S.st->phase = PH_ERR;
+                                cphase = PH_ERR;
+                            }
+                        }
+                        if (cphase >= PH_DONE) continue;
+                        const unsigned i0 = (unsigned)it.y * TV;
+                        P = c.P;
+                        src = static_cast<const T *>(c.A) + i0;
+                        bytes = ((unsigned)min(TV, c.nfluid - i0) * (unsigned)sizeof(T) + 15u) & ~15u;
+                        d.A = c.A;
+                        d.n = c.n;
+                        d.tile_start = i0;
+                        d.solve = it.x;
+                        d.red = cred;
+                        d.P = P;
+                        d.nfluid = c.nfluid;
+                        d.scale = c.scale;
+                        d.inv_scale = c.inv_scale;
+                        d.phys = c.phys;
+                        break;
+                    }
+                    more = w < nwork;
+                    next = more ? w + gridDim.x : w;
+                    d.item = more ? w : -1;
+                    if (more && bytes) {
+                        fence_proxy_async_smem();
+                        mbar_arrive_expect_tx(&full[s], Q3 * bytes);
+                        copies |= 1u << s;
+                    } else {
+                        mbar_arrive(&full[s]);   // end of the list, or an item without voxels
+                    }
+                    fparity ^= 1u << s;
+                }
             }
-            const bool more = w < nwork;
-            next = more ? w + gridDim.x : w;
-            d.item = more ? w : -1;
-            if (more && bytes) {
+            // lane 0's decisions to the warp
+            gave_up = __shfl_sync(0xffffffffu, gave_up ? 1 : 0, 0) != 0;
+            if (gave_up) break;
+            more = __shfl_sync(0xffffffffu, more ? 1 : 0, 0) != 0;
+            bytes = __shfl_sync(0xffffffffu, bytes, 0);
+            P = __shfl_sync(0xffffffffu, P, 0);
+            src = reinterpret_cast<const T *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(src), 0));
+            if (more && bytes && lane < (unsigned)Q3) {
                 unsigned char *buf = ring + s * (Q3 * RUN);
                 fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&full[s], Q3 * bytes);
-#pragma unroll 1
-                for (int k = 0; k < Q3; ++k) bulk_load(buf + k * RUN, src + (size_t)k * P, bytes, &full[s]);
-                copies |= 1u << s;
-            } else {
-                mbar_arrive(&full[s]);   // end of the list, or an item without voxels
+                bulk_load(buf + lane * RUN, src + (size_t)lane * P, bytes, &full[s]);
             }
-            fparity ^= 1u << s;
             if (!more) return;           // the consumers stop at this buffer
         }
         // gave up on a release: wait for the copies still in flight, then leave
-        for (int r = 0; r < NS; ++r)
-            if ((copies >> r) & 1u) mbar_wait_bounded(&full[r], ((fparity >> r) & 1u) ^ 1u, wait_ns);
+        if (lane == 0)
+            for (int r = 0; r < NS; ++r)
+                if ((copies >> r) & 1u) mbar_wait_bounded(&full[r], ((fparity >> r) & 1u) ^ 1u, wait_ns);
         return;
     }
 
@@ -937,7 +1000,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
         const int phase = S.st->phase;
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
-        const bool red = needs_reduction(S.c, phase, n);
+        const bool red = step_reduces(a, S.c, phase, n);
         T *__restrict__ A = static_cast<T *>(S.A);
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
@@ -1017,7 +1080,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_group_kernel(const Step
             const int phase = S.st->phase;
             if (phase >= PH_DONE) continue;
             live |= 1u << d;
-            if (needs_reduction(S.c, phase, S.st->s_base + a.step + 1)) {
+            if (step_reduces(a, S.c, phase, S.st->s_base + a.step + 1)) {
                 redm |= 1u << d;
                 sacc[d][0][threadIdx.x] = 0.0;
                 sacc[d][1][threadIdx.x] = 0.0;
@@ -1145,7 +1208,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_links_kernel(const Step
             if (!((live >> d) & 1u)) continue;
             const Solve3 &S = a.solves[item.x + d];
             const long long n = S.st->s_base + a.step + 1;
-            const bool red = needs_reduction(S.c, S.st->phase, n);
+            const bool red = step_reduces(a, S.c, S.st->phase, n);
             T *__restrict__ A = static_cast<T *>(S.A);
             double acc[3] = {0.0, 0.0, 0.0};
             if constexpr (PAIR) {
@@ -1197,6 +1260,92 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_links_kernel(const Step
     }
 }
 
+// The link-slot even step with one voxel per thread: blocks of 2 * TPB
+// threads, thread t stepping voxel t of the tile.  A tile's directions take
+// half as long per block as with two voxels per thread, so the grouped work
+// list (a third as many items as the per-direction one) spreads over the
+// SMs in more, shorter waves.  On reduction steps the velocities pass
+// through shared memory so that thread t < TPB sums voxel t, then voxel
+// t + TPB, as the other kernels do (the same flux bits); threads t >= TPB
+// take no part in the block sum (named barrier 1 over the first TPB threads).
+template <class ST, int MINB, bool W1, bool META>
+__global__ void __launch_bounds__(2 * TPB, MINB) step3d_even_links1_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    using Cp = typename ST::C;
+    static_assert(TILE_NPT == 2, "a tile is one voxel per thread of a 2 * TPB block");
+    constexpr unsigned TV = TPB * TILE_NPT;
+    __shared__ double sh[TPB / 32][3];
+    __shared__ unsigned sl[Q3 - 1][TV];
+    __shared__ float su[3][TV];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    const unsigned tid = threadIdx.x;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S0 = a.solves[item.x];
+        const int ng = min(S0.group, MAX_GROUP);
+        unsigned live = 0;
+#pragma unroll
+        for (int d = 0; d < MAX_GROUP; ++d)
+            if (d < ng && a.solves[item.x + d].st->phase < PH_DONE) live |= 1u << d;
+        if (!live) continue;
+        const unsigned P = (unsigned)S0.plane;
+        const unsigned nf = (unsigned)S0.nfluid;
+        const unsigned i0 = (unsigned)item.y * TV;
+        const unsigned i = i0 + tid;
+        const bool v = i < nf;
+        if (v) {
+            CNb nb;
+            if constexpr (META) {
+                meta_nbrs(S0, i, __ldg(S0.meta + i), __ldg(S0.meta2 + i), nb);
+            } else {
+                int x, y, z;
+                coords3(S0, __ldg(S0.fnode + i), x, y, z);
+                compact_nbrs(S0, i, x, y, z, nb);
+            }
+#pragma unroll
+            for (int k = 1; k < Q3; ++k) {
+                const int o = opp3(k);
+                sl[k - 1][tid] = ((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]);
+            }
+        }
+#pragma unroll 1
+        for (int d = 0; d < ng; ++d) {
+            if (!((live >> d) & 1u)) continue;
+            const Solve3 &S = a.solves[item.x + d];
+            const long long n = S.st->s_base + a.step + 1;
+            const bool red = step_reduces(a, S.c, S.st->phase, n);
+            T *__restrict__ A = static_cast<T *>(S.A);
+            Cp ux = Cp(0), uy = Cp(0), uz = Cp(0);
+            if (v) {
+                Cp g[Q3];
+                g[0] = ST::ld(A + i);
+#pragma unroll
+                for (int k = 1; k < Q3; ++k) g[k] = ST::ld(A + sl[k - 1][tid]);
+                collide3<ST, W1>(g, S, ux, uy, uz);
+                const uint32_t hv = voxel_bits<ST>(i, n);
+                store_pop<ST>(A, i, g[0], hv, 0);
+#pragma unroll
+                for (int k = 1; k < Q3; ++k) store_pop<ST>(A, sl[opp3(k) - 1][tid], g[k], hv, k);
+            }
+            if (red) {
+                su[0][tid] = (float)ux; su[1][tid] = (float)uy; su[2][tid] = (float)uz;
+                __syncthreads();
+                if (tid < TPB) {
+                    double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        if (i < nf) acc[c] += (double)su[c][tid];
+                        if (i + TPB < nf) acc[c] += (double)su[c][tid + TPB];
+                    }
+                    finish_tile<TPB, 1>(S, item.y, n, acc, sh, defer_slot(a));
+                }
+                __syncthreads();      // su and sh are reused by the next direction
+            }
+        }
+    }
+}
+
 // Even step with its gathers staged in shared memory by cp.async: the pulls
 // of all TILE_NPT voxels of a thread are issued (address from the neighbour
 // record, copy straight to shared memory, no register held) before the first
@@ -1218,7 +1367,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const Step
         const int phase = S.st->phase;
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
-        const bool red = needs_reduction(S.c, phase, n);
+        const bool red = step_reduces(a, S.c, phase, n);
         T *__restrict__ A = static_cast<T *>(S.A);
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
@@ -1286,10 +1435,11 @@ __global__ void build_meta_kernel(Solve3 S, uint4 *meta, uint2 *meta2);
 __global__ void advance3d_kernel(Solve3 *solves, int nsolves, long long steps);
 
 // Deferred reduction of the launches with relative steps step0 .. step0 +
-// nsteps - 1 (nsteps <= DEFER_SLOTS): the fluxes (qbuf: per solve and step,
-// q[3] and a flag), then the controllers in step order.
+// nsteps - 1 (nsteps <= DEFER_SLOTS, within one block of DEFER_SLOTS): the
+// fluxes (qbuf: per solve and step, q[3] and a flag), then the controllers
+// in step order.  mode: StepArgs::defer of those launches.
 cudaError_t launch_deferred3d(const Solve3 *solves, int nsolves, long long step0, int nsteps, double *qbuf,
-                              cudaStream_t s);
+                              int mode, cudaStream_t s);
 
 // Initial state: every population at rest (f = w, or h = 0 when shifted).
 template <class ST>

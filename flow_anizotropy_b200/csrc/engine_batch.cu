@@ -54,6 +54,9 @@ struct lbm_batch {
     int cap_work = 0;
     int nwork = 0;         // items in the device work list (= blocks per step launch)
     int graph_nwork = -1;  // launch size the graph holds
+    int slot_hi = 0;       // slots below this index hold every resident solve
+    int graph_slot_hi = -1;
+    DevMem d_qbuf{nullptr};   // deferred reduction: q and flag per slot and step
     std::vector<Slot> slots;
     DevMem d_solves{nullptr}, d_states{nullptr}, d_work{nullptr}, d_nwork{nullptr};
     cudaGraph_t graph = nullptr;
@@ -81,14 +84,25 @@ static int capture(lbm_batch *b)
     a.nwork_dev = static_cast<const int *>(b->d_nwork.p);
     a.nwork = 0;
     const dim3 grid(std::max(1, b->nwork));
+    const bool defer = lbm_defers(b->precision);
+    a.defer = defer ? 2 : 0;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     // chunks are even and solves join at chunk boundaries (s_base even), so
-    // launch i runs step i + 1 of every solve: odd launches use the local kernel
+    // launch i runs step i + 1 of every solve: odd launches use the local kernel.
+    // Deferred reduction: a pass after every DEFER_SLOTS launches and at the
+    // chunk's end; solves sit at different step counts, so their phases can
+    // change inside a pass (mode 2)
     for (int i = 0; i < b->chunk && e == cudaSuccess; ++i) {
         a.step = i;
         const bool odd = ((i + 1) & 1) == 1;
         e = lbm_launch_step(b->precision, b->variant, b->w1, odd, grid, ctx->stream, a);
+        const bool pass_end = ((i + 1) % DEFER_SLOTS) == 0 || i + 1 == b->chunk;
+        if (e == cudaSuccess && defer && pass_end) {
+            const int first = i - (i % DEFER_SLOTS);
+            e = launch_deferred3d(static_cast<const Solve3 *>(b->d_solves.p), std::max(1, b->slot_hi), first,
+                                  i + 1 - first, static_cast<double *>(b->d_qbuf.p), 2, ctx->stream);
+        }
     }
     if (e == cudaSuccess) {
         advance3d_kernel<<<(b->cap_slots + 255) / 256, 256, 0, ctx->stream>>>(
@@ -105,6 +119,7 @@ static int capture(lbm_batch *b)
             if (b->graph) cudaGraphDestroy(b->graph);
             b->graph = g;
             b->graph_nwork = b->nwork;
+            b->graph_slot_hi = b->slot_hi;
             return LBM_OK;
         }
         cudaGetLastError();            // not updatable (kernels changed): instantiate anew
@@ -113,6 +128,7 @@ static int capture(lbm_batch *b)
     b->graph = g;
     CK(cudaGraphInstantiate(&b->exec, g, 0));
     b->graph_nwork = b->nwork;
+    b->graph_slot_hi = b->slot_hi;
     return LBM_OK;
 }
 
@@ -122,6 +138,10 @@ static int sync_work(lbm_batch *b)
     lbm_ctx *ctx = b->ctx;
     std::vector<Solve3> desc(b->cap_slots);
     std::vector<int2> work;
+    int hi = 0;
+    for (int i = 0; i < b->cap_slots; ++i)
+        if (b->slots[i].used) hi = i + 1;
+    b->slot_hi = hi;
     for (int i = 0; i < b->cap_slots; ++i) {
         const Slot &s = b->slots[i];
         if (!s.used) {
@@ -135,7 +155,7 @@ static int sync_work(lbm_batch *b)
             for (int t = 0; t < s.S.ntiles; ++t) work.push_back(make_int2(i, t));
     }
     const int nwork = (int)work.size();
-    bool recapture = nwork != b->graph_nwork;
+    bool recapture = nwork != b->graph_nwork || b->slot_hi != b->graph_slot_hi;
     if (nwork > b->cap_work) {
         b->cap_work = std::max<int>(nwork, 2 * b->cap_work);
         CK(b->d_work.alloc(sizeof(int2) * (size_t)b->cap_work));
@@ -167,7 +187,7 @@ extern "C" long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int pre
         return tables + md_pmask_bytes(g, ny, nz) + (long long)ndir * (md_lattice_bytes(g) + 24ll * tiles);
     }
     const long long tiles = (nn + TPB - 1) / TPB;
-    return tables + (long long)ndir * (lbm_lattice_bytes3d(nn, precision) + 24 * tiles);
+    return tables + (long long)ndir * (lbm_lattice_bytes3d(nn, precision) + 8 * lbm_partial_doubles(precision, (int)tiles));
 }
 
 extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, long long hbm_budget, int chunk)
@@ -184,7 +204,7 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     b->precision = precision;
     b->chunk = chunk;
     b->budget = hbm_budget;
-    b->variant = lbm_default_variant(precision);
+    b->variant = lbm_default_batch_variant(precision);
     b->npt = variant_npt(precision, b->variant);
     b->cap_slots = 4096;
     b->cap_work = 1 << 16;
@@ -199,6 +219,8 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     CK(b->d_states.alloc(sizeof(State3) * b->cap_slots));
     CK(b->d_work.alloc(sizeof(int2) * b->cap_work));
     CK(b->d_nwork.alloc(sizeof(int)));
+    b->d_qbuf = DevMem(ctx->stream);
+    CK(b->d_qbuf.alloc(sizeof(double) * 4 * DEFER_SLOTS * (size_t)b->cap_slots));
     std::vector<State3> done(b->cap_slots);
     for (auto &st : done) { memset(&st, 0, sizeof(st)); st.phase = PH_DONE; }
     CK(cudaMemcpyAsync(b->d_states.p, done.data(), sizeof(State3) * b->cap_slots, cudaMemcpyHostToDevice, ctx->stream));
@@ -212,7 +234,7 @@ extern "C" int lbm_batch_set_variant(lbm_batch *b, int variant)
 {
     if (!b) return LBM_EINPUT;
     lbm_ctx *ctx = b->ctx;
-    if (variant == LBM_VARIANT_DEFAULT) variant = lbm_default_variant(b->precision);
+    if (variant == LBM_VARIANT_DEFAULT) variant = lbm_default_batch_variant(b->precision);
     if (variant < 0 || variant >= variant_count(b->precision))
         return lbm_fail_input(ctx, "unknown step-kernel variant");
     for (const Slot &s : b->slots)
@@ -276,7 +298,8 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
     const long long tables = 4ll * ((nx + 31) / 32) * (long long)ny * nz * 2 + 4ll * proto.nfluid + 8 +
                              (proto.meta ? 24ll * proto.nfluid : 0) +
                              (is_dense_m(b->precision) ? md_pmask_bytes(proto.md, ny, nz) : 0);
-    const long long exact = tables + (long long)ndir * (lbm_lattice_bytes(proto) + 24ll * proto.ntiles);
+    const long long part_bytes = 8ll * lbm_partial_doubles(b->precision, proto.ntiles);
+    const long long exact = tables + (long long)ndir * (lbm_lattice_bytes(proto) + part_bytes);
     if (b->resident + exact > b->budget) {
         ctx->err = "batch budget exhausted";
         return LBM_EBUSY;
@@ -295,7 +318,7 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         s.wpre = wpre; s.fnode = fnode; s.meta = meta; s.meta2 = meta2;
         s.tables = tables;
         CK(s.lattice.alloc((size_t)lbm_lattice_bytes(s.S)));
-        CK(s.partials.alloc(sizeof(double) * 3 * (size_t)s.S.ntiles));
+        CK(s.partials.alloc(sizeof(double) * (size_t)lbm_partial_doubles(b->precision, s.S.ntiles)));
         s.S.A = s.lattice.p;
         s.S.mask = static_cast<const uint32_t *>(mask->p);
         s.S.partials = static_cast<double *>(s.partials.p);
@@ -305,7 +328,7 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         s.dir = j;
         s.used = true;
         s.retired = false;
-        s.bytes = lbm_lattice_bytes(s.S) + 24ll * s.S.ntiles;
+        s.bytes = lbm_lattice_bytes(s.S) + part_bytes;
         lbm_init_state3(init[j], s.S.c);
         CK(lbm_init_lattice(b->precision, s.S, ctx->stream));
         CK(cudaMemcpyAsync(s.S.st, &init[j], sizeof(State3), cudaMemcpyHostToDevice, ctx->stream));

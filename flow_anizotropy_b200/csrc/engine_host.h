@@ -23,6 +23,11 @@ int lbm_fail_cuda(lbm_ctx *ctx, cudaError_t e, const char *what, int line);
 int lbm_fail_input(lbm_ctx *ctx, const std::string &msg);
 // The step-kernel variant LBM_VARIANT_DEFAULT stands for.
 int lbm_default_variant(int prec);
+int lbm_default_batch_variant(int prec);
+// Deferred flux reduction (StepArgs::defer) for this precision, and the
+// doubles of a solve's partials buffer with it.
+bool lbm_defers(int prec);
+long long lbm_partial_doubles(int prec, int ntiles);
 bool lbm_is_device_ptr(const void *p);
 std::string &lbm_last_error_global();
 

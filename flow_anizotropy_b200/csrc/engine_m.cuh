@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(TPB, MINB) stepm_kernel(const StepArgs a)
         const int phase = S.st->phase;
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
-        const bool red = needs_reduction(S.c, phase, n);
+        const bool red = step_reduces(a, S.c, phase, n);
         char *base = static_cast<char *>(S.A);
         const long long slots = S.plane;
         const long long bytes = slots * (long long)MT::rec_bytes;

@@ -16,6 +16,7 @@ int max_blocks_f64(int variant, bool odd);
 #define LBM_EVENA(ST, V, W) step3d_even_async_kernel<ST, even_lp(V).minb, W>
 #define LBM_EVENG(ST, V, W) step3d_even_group_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 #define LBM_EVENL(ST, V, W) step3d_even_links_kernel<ST, even_lp(V).minb, W, even_meta(V), even_pair(V)>
+#define LBM_EVENW(ST, V, W) step3d_even_links1_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 #define LBM_ODDB(ST, W) step3d_odd_bulk_kernel<ST, odd_lp(4).minb, W>
 
 // Persistent CTAs of the bulk-staged odd kernel per (storage, tau = 1, device),
@@ -87,7 +88,9 @@ static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const S
         case 9: LBM_EVENL(ST, 9, W)<<<grid, TPB, 0, s>>>(a); break;
         case 10: LBM_EVENL(ST, 10, W)<<<grid, TPB, 0, s>>>(a); break;
         case 11: LBM_EVENL(ST, 11, W)<<<grid, TPB, 0, s>>>(a); break;
-        default: LBM_EVENL(ST, 12, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 12: LBM_EVENL(ST, 12, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 13: LBM_EVENW(ST, 13, W)<<<grid, 2 * TPB, 0, s>>>(a); break;
+        default: LBM_EVENW(ST, 14, W)<<<grid, 2 * TPB, 0, s>>>(a); break;
         }
     }
     return cudaGetLastError();
@@ -120,9 +123,10 @@ static int occ(int v, bool odd)
                            : ve == 6 ? (const void *)LBM_EVENG(ST, 6, true) : ve == 7 ? (const void *)LBM_EVENG(ST, 7, true)
                            : ve == 8 ? (const void *)LBM_EVENL(ST, 8, true) : ve == 9 ? (const void *)LBM_EVENL(ST, 9, true)
                            : ve == 10 ? (const void *)LBM_EVENL(ST, 10, true) : ve == 11 ? (const void *)LBM_EVENL(ST, 11, true)
-                           : (const void *)LBM_EVENL(ST, 12, true));
+                           : ve == 12 ? (const void *)LBM_EVENL(ST, 12, true) : ve == 13 ? (const void *)LBM_EVENW(ST, 13, true)
+                           : (const void *)LBM_EVENW(ST, 14, true));
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, TPB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, (!odd && even_wide(ve)) ? 2 * TPB : TPB, 0);
     return nb;
 }
 

@@ -43,7 +43,10 @@ extern "C" {
 
 /* lbm_params3d.variant: the library's default for the precision (the
  * variant the autotuner picks on the 128^3 tensor workload: FP32 3, FP16 and
- * BF16 33, 0 otherwise).  Every variant of a precision gives the same bits. */
+ * BF16 71, 0 otherwise; a batch, which steps each direction on its own,
+ * defaults to FP16 and BF16 61).  Every variant of a precision gives the same
+ * bits.  Variant v runs odd-step kernel v / 15 and even-step kernel v % 15
+ * for FP32, FP16 and BF16 (v / 6 and v % 6 for FP64). */
 #define LBM_VARIANT_DEFAULT (-1)
 
 /* Population storage (collision arithmetic is FP64 for LBM_FP64, else FP32;
@@ -200,8 +203,8 @@ int  lbm_batch_create(lbm_ctx *ctx, lbm_batch **batch, int precision,
                       long long hbm_budget, int chunk);
 
 /* Step-kernel variant of every launch of an empty batch (default
- * LBM_VARIANT_DEFAULT, the variant lbm_tune3d picks on the 128^3 tensor
- * workload; mixes of small structures may prefer another).  Results do not
+ * LBM_VARIANT_DEFAULT, the best per-direction variant lbm_tune3d finds on the
+ * 128^3 tensor workload; mixes of small structures may prefer another).  Results do not
  * depend on it.  LBM_EINPUT while solves are resident, and for the grouped
  * even-step variants (they step all directions of a structure in one work
  * item; the batch steps each direction on its own). */

@@ -16,7 +16,7 @@ from flow_anizotropy_b200 import structures as st
 
 pytestmark = pytest.mark.gpu
 
-NV_EVEN = 13          # even variants per odd variant (NVAR_EVEN_LP)
+NV_EVEN = 15          # even variants per odd variant (NVAR_EVEN_LP)
 PAIR, BULK = 3, 4          # odd variant indices
 
 
@@ -100,7 +100,8 @@ def test_starved_waits_end_with_status(gpu):
     assert rc == rc0 and ok[0].steps == ref[0].steps and np.array_equal(ok[0].q, ref[0].q)
 
 
-@pytest.mark.parametrize("prec,default", [("fp32", 3), ("fp16", 33), ("bf16", 33), ("fp64", 0)])
+@pytest.mark.parametrize("prec,default", [("fp32", 3), ("fp16", 4 * NV_EVEN + 11), ("bf16", 4 * NV_EVEN + 11),
+                                          ("fp64", 0)])
 def test_default_variant_is_the_tuned_pick_and_matches_variant_0(gpu, prec, default):
     """LBM_VARIANT_DEFAULT runs the listed variant; since every variant sums
     the fluxes in one order, a whole solve with it equals variant 0's bits."""

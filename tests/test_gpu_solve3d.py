@@ -78,7 +78,7 @@ def test_grouped_even_step_equals_per_direction(gpu, packing, prec, ndir):
     direction (a group of one after a group of three) and a single one."""
     F = 1e-6
     forces = [[F, 0, 0], [0, F, 0], [0, 0, F], [F / 3**0.5] * 3][:ndir]
-    nv_even = 13      # NVAR_EVEN_LP
+    nv_even = 15      # NVAR_EVEN_LP
     runs = {}
     for ve in (2, 3, 6, 7):
         p = S.Params3D(precision=prec, variant=ve, **PRM)

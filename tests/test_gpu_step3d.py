@@ -103,7 +103,7 @@ def test_every_odd_variant_agrees_general_tau(gpu, prec):
     solid = _solid((10, 13, 37), 23)
     force = [-4e-7, 2e-7, 1e-6]
     nv = _lib.load().lbm_variant_count(_lib.PRECISIONS[prec])
-    nv_even = 13      # NVAR_EVEN_LP
+    nv_even = 15      # NVAR_EVEN_LP
     ref = {n: debug_steps3d(solid, force, n, tau=0.8, precision=prec, variant=1) for n in (3, 4)}
     for vo in range(1, nv // nv_even):
         for n in (3, 4):
