@@ -29,7 +29,10 @@ Reported (one JSON line, rank 0):
              q / phi of each forcing direction;
   serving    the continuous-batching server on the serving mix (batch-mix
              structures, one 256^3 GRF in every 20 requests) at 20 requests/s
-             for --serve-seconds, p50/p99 latency of what completed;
+             for --serve-seconds, p50/p99 latency of what completed (that rate
+             overloads one GPU, so these latencies are mostly queueing), and
+             `sustained`: the same mix at --serve-sustained of the rate served,
+             every request run to completion, p50/p99 of all of them;
   large      512^3 GRF, tau 0.8, fixed steps: GLUPS and roofline per path;
   batch      a sample of the 256-structure uneven-size mix, batched against
              one structure at a time in plain FP32;
@@ -339,6 +342,24 @@ def serve_trace(device, prec, args):
     queued, resident = len(srv.queue), len(srv.inflight)
     srv.close()
     served = stats.completed / wall
+    # the same mix at a load the GPU sustains (a fraction of the rate just
+    # served): every request runs to completion, so p50/p99 are the solver's
+    # latency under continuous batching rather than the overloaded queue's
+    sus = None
+    if args.serve_sustained > 0 and served > 0:
+        rate2 = args.serve_sustained * served
+        srv2 = Server(precision=prec, hbm_budget=150 * 2**30, chunk=128, device=device, variant=args.serve_variant)
+        arr2 = poisson_arrivals(rate2, args.serve_seconds, seed=12)
+        t0 = time.perf_counter()
+        st2 = replay(srv2, arr2, request)
+        wall2 = time.perf_counter() - t0
+        srv2.close()
+        lat2 = np.array(st2.latencies) if st2.latencies else np.array([np.nan])
+        sus = {"rate_per_s": rate2, "load_fraction": args.serve_sustained, "arrival_seconds": args.serve_seconds,
+               "arrived": len(arr2), "completed": st2.completed, "wall_seconds": wall2,
+               "p50_s": float(np.percentile(lat2, 50)), "p99_s": float(np.percentile(lat2, 99)),
+               "p50_queue_s": float(np.percentile(st2.queue_waits, 50)) if st2.queue_waits else None,
+               "max_resident": st2.max_resident, "k_tensors_per_hr": 3600.0 * st2.completed / wall2}
     # plain FP32, one structure at a time with the library's default FP32
     # kernels, on a sample of the same mix weighted as the stream is (19 mix
     # requests to 1 GRF)
@@ -368,7 +389,8 @@ def serve_trace(device, prec, args):
                    f"and {len(grf)} 256^3 GRF samples (every 20th request)",
             "path": prec, "batch_variant": args.serve_variant,
             "latency_note": "latencies of the requests completed within the window (an overloaded "
-                            "server's queue grows without bound, so they understate the steady state)"}
+                            "server's queue grows without bound, so they understate the steady state)",
+            "sustained": sus}
 
 
 # -------------------------------------------------------------- our arm ----
@@ -815,7 +837,9 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp16", "bf16", "fp32", "fp64", "m32", "md32"])
     ap.add_argument("--serve-seconds", type=float, default=120.0,
                     help="arrival window of the serving leg (0: no serving leg)")
-    ap.add_argument("--serve-precision", default="bf16", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--serve-precision", default="fp16", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--serve-sustained", type=float, default=0.7,
+                    help="serving: second trace at this fraction of the served rate, run to completion (0: none)")
     ap.add_argument("--serve-variant", type=int, default=-1,
                     help="step-kernel variant of the serving batch (-1: library default)")
     ap.add_argument("--serve-pool", type=int, default=40, help="distinct batch-mix structures the requests draw")
@@ -836,7 +860,7 @@ def main():
     ap.add_argument("--gen-size", type=int, default=80, help="cell edge of the gen3d workload")
     ap.add_argument("--count", type=int, default=48,
                     help="structures of the batch leg / workload (0: no batch leg)")
-    ap.add_argument("--batch-paths", default="bf16")
+    ap.add_argument("--batch-paths", default="fp16")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

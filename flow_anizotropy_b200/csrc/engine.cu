@@ -171,12 +171,13 @@ int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
     return LBM_OK;
 }
 
-// The autotuner's pick on the 128^3 tensor workload: FP32 plain odd + even
-// ranks from the mask; 16-bit bulk-staged odd + grouped even step with the
-// link slots shared by the directions and voxel pairs collided together.
+// The autotuner's pick on the 128^3 tensor workload: FP32 the pull form
+// (voxel pairs, ranks from the neighbour record, 3 blocks per SM); 16-bit
+// bulk-staged odd + grouped even step with the link slots shared by the
+// directions and voxel pairs collided together.
 int lbm_default_variant(int prec)
 {
-    if (prec == LBM_FP32) return 0 * NVAR_EVEN_LP + 3;
+    if (prec == LBM_FP32) return NVAR_LP + 1;
     if (prec == LBM_FP16 || prec == LBM_BF16) return 4 * NVAR_EVEN_LP + 11;
     return 0;
 }
@@ -206,10 +207,20 @@ long long lbm_lattice_bytes3d(long long n, int prec)
     return (long long)Q3 * lbm_plane_elems(n) * (long long)elem_size(prec);
 }
 
-// Lattice bytes of one direction of a filled solve record.
+// Lattice bytes of one direction of a filled solve record (both lattices of
+// the pull form).
 long long lbm_lattice_bytes(const Solve3 &S)
 {
-    return is_dense_m(S.prec) ? md_lattice_bytes(S.md) : lbm_lattice_bytes3d(S.nfluid, S.prec);
+    if (is_dense_m(S.prec)) return md_lattice_bytes(S.md);
+    return lbm_lattice_bytes3d(S.nfluid, S.prec) * (S.pull ? 2 : 1);
+}
+
+// Point a solve record at its lattice memory (lbm_lattice_bytes(S) bytes);
+// the pull form's second lattice follows the first.
+void lbm_attach_lattice(Solve3 &S, void *p)
+{
+    S.A = p;
+    S.B = S.pull ? static_cast<char *>(p) + lbm_lattice_bytes3d(S.nfluid, S.prec) : nullptr;
 }
 
 // Plane stride (populations) or record slots per buffer (moments).
@@ -222,6 +233,8 @@ long long lbm_plane_for(int prec, long long n)
 int lbm_effective_variant(int prec, int variant, bool have_meta)
 {
     if (is_moment(prec) || is_dense_m(prec) || have_meta) return variant;
+    if (is_pull_variant(prec, variant))
+        return pull_meta(variant - NVAR_LP) ? NVAR_LP + 2 : variant;   // pull, ranks from the mask
     const int ve = variant % nvar_even(prec);
     if (!even_meta(ve)) return variant;
     if (even_wide(ve)) return variant - ve + 14;        // link slots, one voxel per thread, ranks from the mask
@@ -231,9 +244,16 @@ int lbm_effective_variant(int prec, int variant, bool have_meta)
 }
 
 // Does this (effective) variant run the grouped even kernel?
-static bool lbm_grouped_variant(int prec, int variant)
+bool lbm_grouped_variant(int prec, int variant)
 {
+    if (is_pull_variant(prec, variant)) return pull_grouped(variant - NVAR_LP);
     return prec >= LBM_FP32 && prec <= LBM_BF16 && even_grouped(variant % NVAR_EVEN_LP);
+}
+
+// Do all launches (not only the even ones) of this variant take the grouped work list?
+static bool lbm_grouped_all(int prec, int variant)
+{
+    return is_pull_variant(prec, variant) && pull_grouped(variant - NVAR_LP);
 }
 
 // Work list of the grouped even step over solves that share one structure:
@@ -280,6 +300,7 @@ void lbm_fill_solve3(Solve3 &S, int nx, int ny, int nz, const double F[3], const
 {
     memset(&S, 0, sizeof(S));
     S.prec = p.precision;
+    S.pull = is_pull_variant(p.precision, p.variant) ? 1 : 0;
     S.nx = nx; S.ny = ny; S.nz = nz;
     S.wpr = (nx + 31) / 32;
     S.nn = (long long)nx * ny * nz;
@@ -454,8 +475,9 @@ static int run_plain3d(lbm_ctx *ctx, std::vector<Solve3> &hs, Solve3 *d_solves, 
     a.starve = ctx->test_starve;
     ae.wait_ns = a.wait_ns;
     ae.starve = a.starve;
+    const bool gall = lbm_grouped_all(prec, variant);
     auto launch = [&](long long rel, bool odd) {
-        StepArgs x = odd ? a : ae;
+        StepArgs x = (odd && !gall) ? a : ae;
         x.step = rel;
         return lbm_launch_step(prec, variant, w1, odd, dim3(x.nwork), ctx->stream, x);
     };
@@ -567,7 +589,7 @@ extern "C" int lbm_solve3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, i
         part.emplace_back(ctx->stream);
         CK(lat.back().alloc((size_t)lbm_lattice_bytes(S)));
         CK(part.back().alloc(sizeof(double) * (size_t)lbm_partial_doubles(prec, S.ntiles)));
-        S.A = lat.back().p;
+        lbm_attach_lattice(S, lat.back().p);
         S.mask = static_cast<const uint32_t *>(mask.p);
         S.partials = static_cast<double *>(part.back().p);
         S.st = static_cast<State3 *>(d_states.p) + j;
@@ -668,7 +690,8 @@ extern "C" int lbm_debug_steps3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int
     CK(lat.alloc((size_t)lbm_lattice_bytes(S)));
     CK(part.alloc(sizeof(double) * (size_t)lbm_partial_doubles(precision, S.ntiles)));
     CK(d_states.alloc(sizeof(State3)));
-    S.A = lat.p; S.mask = static_cast<const uint32_t *>(mask.p);
+    lbm_attach_lattice(S, lat.p);
+    S.mask = static_cast<const uint32_t *>(mask.p);
     S.partials = static_cast<double *>(part.p); S.st = static_cast<State3 *>(d_states.p);
     lbm_init_state3(hst[0], S.c);
     CK(lbm_init_lattice(precision, S, ctx->stream));
@@ -771,7 +794,7 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
             F[j % 3] = 1e-6;
             lbm_fill_solve3(hs[j], nx, ny, nz, F, p, npt);
             lbm_copy_pores(hs[j], proto);
-            hs[j].A = lat[j].p;
+            lbm_attach_lattice(hs[j], lat[j].p);
             hs[j].mask = proto.mask;
             hs[j].partials = static_cast<double *>(part.p) + 3ll * j * max_tiles;
             hs[j].st = static_cast<State3 *>(d_states.p) + j;
@@ -801,9 +824,10 @@ extern "C" int lbm_tune3d(lbm_ctx *ctx, const uint8_t *solid, int nx, int ny, in
             ae.work = static_cast<const int2 *>(gw.p);
             ae.nwork = (int)items.size();
         }
+        const bool gall = lbm_grouped_all(precision, ev);
         auto launch = [&](long long s) {
             const bool odd = ((s + 1) & 1) == 1;
-            StepArgs &x = odd ? a : ae;
+            StepArgs &x = (odd && !gall) ? a : ae;
             x.step = s;
             return lbm_launch_step(precision, ev, true, odd, dim3(x.nwork), ctx->stream, x);
         };

@@ -113,6 +113,7 @@ struct MDGeom {
 
 struct Solve3 {
     void *A;
+    void *B;                 // pull form: the second lattice (else null)
     long long plane;         // elements per plane (>= nfluid)
     const uint32_t *mask;
     const uint32_t *wpre;    // pore voxels before each mask word (+ final total)
@@ -132,6 +133,7 @@ struct Solve3 {
     State3 *st;
     MDGeom md;            // dense moment form only
     int group;            // grouped even step: directions in the group led by this record (else 0)
+    int pull;             // two-lattice pull form (step3d_pull_kernel): A and B alternate
 };
 
 struct StepArgs {
@@ -556,6 +558,20 @@ __host__ __device__ constexpr Variant even_f64(int v)
     return v == 0 ? Variant{1, 2} : v == 1 ? Variant{1, 1} : v == 2 ? Variant{1, 2} : v == 3 ? Variant{1, 1}
          : v == 4 ? Variant{1, 2} : Variant{1, 3};
 }
+// Pull-form variants (two lattices, one kernel for every step; see
+// step3d_pull_kernel) are the reduced-precision indices NVAR_LP ..
+// NVAR_LP + NVAR_PULL - 1; with p = v - NVAR_LP: 0-1 per direction, source
+// ranks from the neighbour record, 2 or 3 blocks per SM; 2 per direction,
+// ranks from the mask; 3 one voxel per thread at a time (voxels t and
+// t + TPB of a tile, one-voxel collision and stores), 4 blocks per SM; 4-5 a
+// structure's directions in one work item with the source slots found once
+// into shared memory (ranks from the record), 2 or 3 blocks per SM.  All but
+// 3 step a thread's two adjacent voxels together.
+constexpr int NVAR_PULL = 6;
+__host__ __device__ constexpr bool is_pull_variant(int prec, int v) { return prec >= 1 && prec <= 3 && v >= NVAR_LP; }
+__host__ __device__ constexpr int pull_minb(int p) { return p == 3 ? 4 : (p == 0 || p == 2 || p == 4) ? 2 : 3; }
+__host__ __device__ constexpr bool pull_meta(int p) { return p != 2; }
+__host__ __device__ constexpr bool pull_grouped(int p) { return p >= 4; }
 // pore voxels per tile: the odd and even kernels of one solve share the tile
 // list (and its partials), so both use TPB * TILE_NPT voxels per tile
 constexpr int TILE_NPT = 2;
@@ -1423,6 +1439,230 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const Step
     }
 }
 
+// ------------------------------------------------------------ pull form ----
+// Two-lattice ("pull") storage of the reduced-precision forms: a direction
+// keeps two lattices of 19 planes (A = buffer 0, B = buffer 1), and step n
+// reads buffer (n - 1) & 1 and writes buffer n & 1.  After step n a buffer
+// holds the post-collision populations in natural slots, f*_k(x_i) at
+// [k][i].  Step n pulls population k of voxel x from [k][rank(x - e_k)], or
+// across a solid link (x - e_k solid) the bounced [opp k][i], collides, and
+// writes all 19 values to its own slots [k][i]: the gathers are the only
+// scattered accesses, the stores are coalesced, and no slot is both read and
+// written in one step (the in-place even step reads and rewrites the same
+// scattered slots).  The initial state is uniform (h = 0), which streaming
+// leaves unchanged, so step 1 (the reference's collide_only priming,
+// LMB3d/lbm3d-perm.cpp:249-253) is an ordinary pull step on it.  The
+// collision, the random bits of every store (voxel, step, direction) and the
+// flux order are those of the in-place kernels, so populations, fluxes and
+// step counts are bit-identical to theirs; the second lattice doubles the
+// memory of a solve.
+//
+// Source slots of the 19 populations of pore voxel i (src[0] = i).
+template <bool META>
+__device__ __forceinline__ void pull_sources(const Solve3 &S, unsigned i, unsigned P, unsigned (&src)[Q3])
+{
+    CNb nb;
+    if constexpr (META) {
+        meta_nbrs(S, i, __ldg(S.meta + i), __ldg(S.meta2 + i), nb);
+    } else {
+        int x, y, z;
+        coords3(S, __ldg(S.fnode + i), x, y, z);
+        compact_nbrs(S, i, x, y, z, nb);
+    }
+    src[0] = i;
+#pragma unroll
+    for (int k = 1; k < Q3; ++k) {
+        const int o = opp3(k);
+        src[k] = ((nb.solid >> o) & 1u) ? (o * P + i) : (k * P + nb.idx[o]);
+    }
+}
+
+// Buffers of step n of a pull-form solve.
+template <class T>
+__device__ __forceinline__ const T *pull_src(const Solve3 &S, long long n)
+{
+    return static_cast<const T *>((n & 1) ? S.A : S.B);
+}
+template <class T>
+__device__ __forceinline__ T *pull_dst(const Solve3 &S, long long n)
+{
+    return static_cast<T *>((n & 1) ? S.B : S.A);
+}
+
+// One step of a pull-form solve: thread t steps the adjacent voxels (2t,
+// 2t + 1) of its tile, gathers both voxels' populations, collides them
+// together in packed FP32 and stores both with paired (4- or 8-byte)
+// coalesced stores.  The partner of the last voxel of an odd-sized lattice is
+// a padding slot of plane stride (read and written, never used).
+template <class ST, int MINB, bool W1, bool META>
+__global__ void __launch_bounds__(TPB, MINB) step3d_pull_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    static_assert(ST::shifted && TILE_NPT == 2, "the pull form is a reduced-precision voxel-pair kernel");
+    constexpr unsigned TV = TPB * TILE_NPT;
+    __shared__ double sh[TPB / 32][3];
+    __shared__ float su[3][TV];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    const unsigned tid = threadIdx.x;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S = a.solves[item.x];
+        const int phase = S.st->phase;
+        if (phase >= PH_DONE) continue;
+        const long long n = S.st->s_base + a.step + 1;
+        const bool red = step_reduces(a, S.c, phase, n);
+        const T *__restrict__ R = pull_src<T>(S, n);
+        T *__restrict__ W = pull_dst<T>(S, n);
+        const unsigned P = (unsigned)S.plane, nf = (unsigned)S.nfluid;
+        const unsigned ts = (unsigned)item.y * TV;
+        const unsigned i0 = ts + 2u * tid;
+        float2 u[3] = {};
+        if (i0 < nf) {
+            unsigned sa[Q3], sb[Q3];
+            pull_sources<META>(S, i0, P, sa);
+            if (i0 + 1u < nf) {
+                pull_sources<META>(S, i0 + 1u, P, sb);
+            } else {
+#pragma unroll
+                for (int k = 0; k < Q3; ++k) sb[k] = k * P + i0 + 1u;
+            }
+            float2 g[Q3];
+            ST::ld2(R + i0, g[0].x, g[0].y);
+#pragma unroll
+            for (int k = 1; k < Q3; ++k) {
+                g[k].x = ST::ld(R + sa[k]);
+                g[k].y = ST::ld(R + sb[k]);
+            }
+            collide3x2<ST, W1>(g, S, u);
+            const uint32_t h0 = voxel_bits<ST>(i0, n), h1 = voxel_bits<ST>(i0 + 1u, n);
+#pragma unroll
+            for (int k = 0; k < Q3; ++k)
+                ST::st2(W + (k * P + i0), g[k].x, g[k].y, dir_bits(h0, k), dir_bits(h1, k));
+        }
+        if (red) {
+            double acc[3];
+            canonical_acc<TPB, 0>(su, u, tid, ts, nf, acc);
+            finish_tile(S, item.y, n, acc, sh, defer_slot(a));
+        }
+    }
+}
+
+// Pull step with one voxel per thread at a time: thread t steps voxels t and
+// t + TPB of its tile one after the other (the flux order of the in-place
+// one-voxel kernels), each with 2- or 4-byte coalesced stores.
+template <class ST, int MINB, bool W1, bool META>
+__global__ void __launch_bounds__(TPB, MINB) step3d_pull1_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    using Cp = typename ST::C;
+    static_assert(ST::shifted, "the pull form is a reduced-precision kernel");
+    __shared__ double sh[TPB / 32][3];
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S = a.solves[item.x];
+        const int phase = S.st->phase;
+        if (phase >= PH_DONE) continue;
+        const long long n = S.st->s_base + a.step + 1;
+        const bool red = step_reduces(a, S.c, phase, n);
+        const T *__restrict__ R = pull_src<T>(S, n);
+        T *__restrict__ W = pull_dst<T>(S, n);
+        const unsigned P = (unsigned)S.plane, nf = (unsigned)S.nfluid;
+        double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int j = 0; j < TILE_NPT; ++j) {
+            const unsigned i = (unsigned)(item.y * (TPB * TILE_NPT) + j * TPB + threadIdx.x);
+            if (i >= nf) continue;
+            unsigned src[Q3];
+            pull_sources<META>(S, i, P, src);
+            Cp g[Q3];
+#pragma unroll
+            for (int k = 0; k < Q3; ++k) g[k] = ST::ld(R + src[k]);
+            Cp ux, uy, uz;
+            collide3<ST, W1>(g, S, ux, uy, uz);
+            const uint32_t hv = voxel_bits<ST>(i, n);
+#pragma unroll
+            for (int k = 0; k < Q3; ++k) store_pop<ST>(W, k * P + i, g[k], hv, k);
+            acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
+        }
+        if (red) finish_tile(S, item.y, n, acc, sh, defer_slot(a));
+    }
+}
+
+// Pull step of a group of directions that share one structure (the grouped
+// work list of the in-place link-slot kernels): the source slots of the
+// tile's voxels are found once into shared memory (each thread reads back
+// only its own, so no barrier) and serve every direction's gathers.  Per
+// direction the arithmetic, random bits and flux order are those of
+// step3d_pull_kernel.
+template <class ST, int MINB, bool W1, bool META>
+__global__ void __launch_bounds__(TPB, MINB) step3d_pull_group_kernel(const StepArgs a)
+{
+    using T = typename ST::T;
+    static_assert(ST::shifted && TILE_NPT == 2, "the pull form is a reduced-precision voxel-pair kernel");
+    constexpr unsigned TV = TPB * TILE_NPT;
+    __shared__ double sh[TPB / 32][3];
+    __shared__ float su[3][TV];
+    __shared__ uint2 sl[Q3 - 1][TPB];            // source slots of population k (1..18) of the thread's pair
+    const int nwork = a.nwork_dev ? *a.nwork_dev : a.nwork;
+    const unsigned tid = threadIdx.x;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const Solve3 &S0 = a.solves[item.x];
+        const int ng = min(S0.group, MAX_GROUP);
+        unsigned live = 0;
+#pragma unroll
+        for (int d = 0; d < MAX_GROUP; ++d)
+            if (d < ng && a.solves[item.x + d].st->phase < PH_DONE) live |= 1u << d;
+        if (!live) continue;
+        const unsigned P = (unsigned)S0.plane, nf = (unsigned)S0.nfluid;
+        const unsigned ts = (unsigned)item.y * TV;
+        const unsigned i0 = ts + 2u * tid;
+        if (i0 < nf) {
+            unsigned sa[Q3], sb[Q3];
+            pull_sources<META>(S0, i0, P, sa);
+            if (i0 + 1u < nf) {
+                pull_sources<META>(S0, i0 + 1u, P, sb);
+            } else {
+#pragma unroll
+                for (int k = 0; k < Q3; ++k) sb[k] = k * P + i0 + 1u;
+            }
+#pragma unroll
+            for (int k = 1; k < Q3; ++k) sl[k - 1][tid] = make_uint2(sa[k], sb[k]);
+        }
+#pragma unroll 1
+        for (int d = 0; d < ng; ++d) {
+            if (!((live >> d) & 1u)) continue;
+            const Solve3 &S = a.solves[item.x + d];
+            const long long n = S.st->s_base + a.step + 1;
+            const bool red = step_reduces(a, S.c, S.st->phase, n);
+            const T *__restrict__ R = pull_src<T>(S, n);
+            T *__restrict__ W = pull_dst<T>(S, n);
+            float2 u[3] = {};
+            if (i0 < nf) {
+                float2 g[Q3];
+                ST::ld2(R + i0, g[0].x, g[0].y);
+#pragma unroll
+                for (int k = 1; k < Q3; ++k) {
+                    const uint2 s = sl[k - 1][tid];
+                    g[k].x = ST::ld(R + s.x);
+                    g[k].y = ST::ld(R + s.y);
+                }
+                collide3x2<ST, W1>(g, S, u);
+                const uint32_t h0 = voxel_bits<ST>(i0, n), h1 = voxel_bits<ST>(i0 + 1u, n);
+#pragma unroll
+                for (int k = 0; k < Q3; ++k)
+                    ST::st2(W + (k * P + i0), g[k].x, g[k].y, dir_bits(h0, k), dir_bits(h1, k));
+            }
+            if (red) {
+                double acc[3];
+                canonical_acc<TPB, 0>(su, u, tid, ts, nf, acc);
+                finish_tile(S, item.y, n, acc, sh, defer_slot(a));
+            }
+        }
+    }
+}
+
 // Pore-rank tables (once per structure).
 constexpr int SCAN_WORDS = 1024;    // mask words per block of the scan kernels
 __global__ void word_sums_kernel(const uint32_t *mask, long long nwords, unsigned *bsum);
@@ -1476,16 +1716,19 @@ __global__ void canon3d_kernel(const Solve3 S, long long done, double *f_out, fl
         CNb nb;
         compact_nbrs(S, i, x, y, z, nb);
         double f[Q3];
+        // pull form: the buffer step `done` wrote holds f*_k at [k][i] (the
+        // initial state, done = 0, sits in A)
+        const T *Ab = S.pull ? static_cast<const T *>((done & 1ll) ? S.B : S.A) : A;
 #pragma unroll
         for (int k = 0; k < Q3; ++k) {
             const int o = opp3(k);
             unsigned at;
-            if (done == 0) at = k * P + i;                          // initial, pre-collision
+            if (done == 0 || S.pull) at = k * P + i;                // initial, pre-collision / pull form
             else if (done & 1ll) at = o * P + i;                    // after a local step
             else if (k == 0) at = i;
             else if ((nb.solid >> k) & 1u) at = o * P + i;
             else at = k * P + nb.idx[k];
-            const double v = (double)ST::ld(A + at);
+            const double v = (double)ST::ld(Ab + at);
             f[k] = ST::shifted ? v * isc + w3(k) : v;
         }
         if (f_out)
@@ -1521,7 +1764,7 @@ inline bool is_dense_m(int prec) { return prec == 6; }
 // shared-memory ring depth x register budget.
 constexpr int NVAR_MD = 4;
 __host__ __device__ constexpr int md_lz(int v) { return v == 1 ? 32 : v == 2 ? 8 : 16; }
-inline int variant_count(int prec) { return prec == 0 ? NVAR_F64 : prec == 6 ? NVAR_MD : (prec >= 4 ? 3 : NVAR_LP); }
+inline int variant_count(int prec) { return prec == 0 ? NVAR_F64 : prec == 6 ? NVAR_MD : (prec >= 4 ? 3 : NVAR_LP + NVAR_PULL); }
 // pore voxels per tile (in units of TPB) of a solve's tile list
 inline int variant_npt(int prec, int) { return prec >= 4 ? 1 : TILE_NPT; }
 

@@ -187,7 +187,9 @@ extern "C" long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int pre
         return tables + md_pmask_bytes(g, ny, nz) + (long long)ndir * (md_lattice_bytes(g) + 24ll * tiles);
     }
     const long long tiles = (nn + TPB - 1) / TPB;
-    return tables + (long long)ndir * (lbm_lattice_bytes3d(nn, precision) + 8 * lbm_partial_doubles(precision, (int)tiles));
+    // the pull form's two lattices, for the precisions that have it
+    const long long lat = lbm_lattice_bytes3d(nn, precision) * (is_pull_variant(precision, NVAR_LP) ? 2 : 1);
+    return tables + (long long)ndir * (lat + 8 * lbm_partial_doubles(precision, (int)tiles));
 }
 
 extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, long long hbm_budget, int chunk)
@@ -240,7 +242,7 @@ extern "C" int lbm_batch_set_variant(lbm_batch *b, int variant)
     for (const Slot &s : b->slots)
         if (s.used) return lbm_fail_input(ctx, "the batch has resident solves");
     if (variant_npt(b->precision, variant) != b->npt) return lbm_fail_input(ctx, "variant changes the tile size");
-    if (b->precision >= LBM_FP32 && b->precision <= LBM_BF16 && even_grouped(variant % NVAR_EVEN_LP))
+    if (lbm_grouped_variant(b->precision, variant))
         return lbm_fail_input(ctx, "grouped even-step variants need a structure's directions in one work item; "
                                    "the batch steps each direction on its own");
     b->variant = variant;
@@ -319,7 +321,7 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         s.tables = tables;
         CK(s.lattice.alloc((size_t)lbm_lattice_bytes(s.S)));
         CK(s.partials.alloc(sizeof(double) * (size_t)lbm_partial_doubles(b->precision, s.S.ntiles)));
-        s.S.A = s.lattice.p;
+        lbm_attach_lattice(s.S, s.lattice.p);
         s.S.mask = static_cast<const uint32_t *>(mask->p);
         s.S.partials = static_cast<double *>(s.partials.p);
         s.S.st = static_cast<State3 *>(b->d_states.p) + free_slots[j];

@@ -77,6 +77,9 @@ int lbm_pick_npt(const lbm_params3d &p);
 int lbm_build_pores(lbm_ctx *ctx, lbm::Solve3 &S, int npt, DevMem &wpre, DevMem &fnode, DevMem &meta,
                     DevMem &meta2);
 int lbm_effective_variant(int prec, int variant, bool have_meta);
+// Does the variant step a structure's directions in one work item (grouped work list)?
+bool lbm_grouped_variant(int prec, int variant);
+void lbm_attach_lattice(lbm::Solve3 &S, void *p);
 void lbm_copy_pores(lbm::Solve3 &dst, const lbm::Solve3 &src);
 cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const lbm::StepArgs &a);
 int lbm_max_blocks(int prec, int variant, bool odd);

@@ -18,6 +18,23 @@ int max_blocks_f64(int variant, bool odd);
 #define LBM_EVENL(ST, V, W) step3d_even_links_kernel<ST, even_lp(V).minb, W, even_meta(V), even_pair(V)>
 #define LBM_EVENW(ST, V, W) step3d_even_links1_kernel<ST, even_lp(V).minb, W, even_meta(V)>
 #define LBM_ODDB(ST, W) step3d_odd_bulk_kernel<ST, odd_lp(4).minb, W>
+#define LBM_PULL(ST, Q, W) step3d_pull_kernel<ST, pull_minb(Q), W, pull_meta(Q)>
+#define LBM_PULL1(ST, Q, W) step3d_pull1_kernel<ST, pull_minb(Q), W, pull_meta(Q)>
+#define LBM_PULLG(ST, Q, W) step3d_pull_group_kernel<ST, pull_minb(Q), W, pull_meta(Q)>
+
+// Pull-form kernel of pull variant q (any step parity).
+template <class ST, bool W>
+static const void *pull_kernel(int q)
+{
+    switch (q) {
+    case 0: return (const void *)LBM_PULL(ST, 0, W);
+    case 1: return (const void *)LBM_PULL(ST, 1, W);
+    case 2: return (const void *)LBM_PULL(ST, 2, W);
+    case 3: return (const void *)LBM_PULL1(ST, 3, W);
+    case 4: return (const void *)LBM_PULLG(ST, 4, W);
+    default: return (const void *)LBM_PULLG(ST, 5, W);
+    }
+}
 
 // Persistent CTAs of the bulk-staged odd kernel per (storage, tau = 1, device),
 // set by prepare_bulk once its shared-memory ring has been allowed.
@@ -61,7 +78,18 @@ static cudaError_t launch_bulk(dim3 grid, cudaStream_t s, const StepArgs &a)
 template <class ST, bool W>
 static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
-    if (v < 0 || v >= NVAR_LP) return cudaErrorInvalidValue;
+    if (v < 0 || v >= NVAR_LP + NVAR_PULL) return cudaErrorInvalidValue;
+    if (v >= NVAR_LP) {
+        switch (v - NVAR_LP) {
+        case 0: LBM_PULL(ST, 0, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 1: LBM_PULL(ST, 1, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 2: LBM_PULL(ST, 2, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 3: LBM_PULL1(ST, 3, W)<<<grid, TPB, 0, s>>>(a); break;
+        case 4: LBM_PULLG(ST, 4, W)<<<grid, TPB, 0, s>>>(a); break;
+        default: LBM_PULLG(ST, 5, W)<<<grid, TPB, 0, s>>>(a); break;
+        }
+        return cudaGetLastError();
+    }
     const int vo = v / NVAR_EVEN_LP, ve = v % NVAR_EVEN_LP;
     if (odd) {
         switch (vo) {
@@ -109,6 +137,11 @@ cudaError_t launch_step3d_lp(int prec, int variant, bool w1, bool odd, dim3 grid
 template <class ST>
 static int occ(int v, bool odd)
 {
+    if (v >= NVAR_LP) {
+        int nb = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pull_kernel<ST, true>(v - NVAR_LP), TPB, 0);
+        return nb;
+    }
     const int vo = v / NVAR_EVEN_LP, ve = v % NVAR_EVEN_LP;
     if (odd && vo == 4) {
         int dev = 0;

@@ -42,11 +42,13 @@ extern "C" {
 #define LBM_ECUDA        (-1)
 
 /* lbm_params3d.variant: the library's default for the precision (the
- * variant the autotuner picks on the 128^3 tensor workload: FP32 3, FP16 and
+ * variant the autotuner picks on the 128^3 tensor workload: FP32 76, FP16 and
  * BF16 71, 0 otherwise; a batch, which steps each direction on its own,
  * defaults to FP16 and BF16 61).  Every variant of a precision gives the same
- * bits.  Variant v runs odd-step kernel v / 15 and even-step kernel v % 15
- * for FP32, FP16 and BF16 (v / 6 and v % 6 for FP64). */
+ * bits.  For FP32, FP16 and BF16, variants v < 75 are the in-place (AA)
+ * lattice, odd-step kernel v / 15 and even-step kernel v % 15; v = 75..80
+ * are the two-lattice pull form (one kernel for every step, twice the
+ * lattice memory).  FP64: odd-step kernel v / 6 and even-step kernel v % 6. */
 #define LBM_VARIANT_DEFAULT (-1)
 
 /* Population storage (collision arithmetic is FP64 for LBM_FP64, else FP32;
@@ -212,8 +214,9 @@ int  lbm_batch_set_variant(lbm_batch *batch, int variant);
 void lbm_batch_destroy(lbm_batch *batch);
 
 /* Upper bound on the device bytes one structure with ndir directions
- * occupies in a batch (as if every voxel were a pore; lattices hold pore
- * voxels only, and admission charges the exact size). */
+ * occupies in a batch (as if every voxel were a pore, and with the pull
+ * form's two lattices for FP32, FP16 and BF16; lattices hold pore voxels
+ * only, and admission charges the exact size of the batch's variant). */
 long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int precision);
 
 /* Admit one structure with ndir directions (results are reported per

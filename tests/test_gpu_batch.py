@@ -102,10 +102,11 @@ def test_batch_variant_choice(gpu):
     from flow_anizotropy_b200 import _lib
     structs = _mix()[:2]
     p = S.Params3D(precision="fp16", **PRM)
-    nve = S.variant_count("fp16") // 5          # even variants per odd variant
+    nve = 15                                    # even variants per odd variant
     pair_meta = 3 * nve + 1                     # odd: voxel pairs; even: neighbour records
+    pull = 5 * nve                              # the two-lattice pull form, per direction
     out = {}
-    for v in (-1, 1, pair_meta):
+    for v in (-1, 1, pair_meta, pull, pull + 3):
         b = S.Batch(precision="fp16", hbm_budget=4 * 2**30, chunk=32, variant=v)
         for t, s in enumerate(structs):
             assert b.submit(s, _forces(), p, tag=t)
@@ -120,7 +121,7 @@ def test_batch_variant_choice(gpu):
                 break
         out[v] = done
         b.close()
-    for v in (1, pair_meta):
+    for v in (1, pair_meta, pull, pull + 3):
         for t in range(len(structs)):
             for a, m in zip(out[-1][t], out[v][t]):
                 assert a.steps == m.steps and np.array_equal(a.q, m.q) and np.array_equal(a.se, m.se), v
@@ -131,4 +132,6 @@ def test_batch_variant_choice(gpu):
     # work item; the batch steps each direction on its own and refuses them
     with pytest.raises(_lib.LBMError, match="grouped"):
         b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, 6))
+    with pytest.raises(_lib.LBMError, match="grouped"):
+        b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, pull + 4))
     b.close()

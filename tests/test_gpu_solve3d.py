@@ -92,7 +92,46 @@ def test_grouped_even_step_equals_per_direction(gpu, packing, prec, ndir):
             assert a.steps == b.steps and a.converged == b.converged
             assert np.array_equal(a.q, b.q) and np.array_equal(a.se, b.se), ve
         assert np.array_equal(vel, vel0), ve
-    assert S.variant_count(prec) == 5 * nv_even
+    assert S.variant_count(prec) == 5 * nv_even + NV_PULL
+
+
+NV_PULL = 6          # pull-form variants after the 5 x 15 in-place ones
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("ndir", [3, 4, 1])
+def test_pull_form_equals_in_place(gpu, packing, prec, ndir):
+    """The two-lattice pull form (one kernel for every step, gathers from the
+    other lattice, coalesced stores to its own) gives the in-place AA
+    kernels' bits over whole solves: step counts, fluxes, standard errors and
+    the exported velocity field, for every pull variant (per direction, one
+    voxel per thread, grouped), also with a group of one after a group of
+    three."""
+    F = 1e-6
+    forces = [[F, 0, 0], [0, F, 0], [0, 0, F], [F / 3**0.5] * 3][:ndir]
+    base = 5 * 15
+    ref, rc0, vel0 = S.solve3d(packing, forces, S.Params3D(precision=prec, variant=1, **PRM), velocity=True)
+    assert ref[0].steps > 0
+    for q in range(NV_PULL):
+        got, rc, vel = S.solve3d(packing, forces, S.Params3D(precision=prec, variant=base + q, **PRM), velocity=True)
+        assert rc == rc0
+        for a, b in zip(ref, got):
+            assert (a.steps, a.converged, a.status) == (b.steps, b.converged, b.status), q
+            assert np.array_equal(a.q, b.q) and np.array_equal(a.se, b.se), q
+        assert np.array_equal(vel, vel0), q
+
+
+def test_pull_form_general_tau(gpu, packing):
+    """tau != 1 (the general operator) in the pull form: the same bits as the
+    in-place kernels over a whole FP16 solve."""
+    F = 1e-6
+    forces = [[0, F, 0], [0, 0, F]]
+    prm = dict(PRM, max_steps=1500)
+    ref, rc0, _ = S.solve3d(packing, forces, S.Params3D(precision="fp16", tau=0.8, variant=1, **prm))
+    for q in (0, 3, 4):
+        got, rc, _ = S.solve3d(packing, forces, S.Params3D(precision="fp16", tau=0.8, variant=75 + q, **prm))
+        for a, b in zip(ref, got):
+            assert a.steps == b.steps and np.array_equal(a.q, b.q) and np.array_equal(a.se, b.se), q
 
 
 def test_batch_means_criterion_on_small_noisy_structure(gpu):

@@ -110,6 +110,12 @@ def test_every_odd_variant_agrees_general_tau(gpu, prec):
             f, u, q = debug_steps3d(solid, force, n, tau=0.8, precision=prec, variant=vo * nv_even + 1)
             assert np.array_equal(f, ref[n][0]) and np.array_equal(u, ref[n][1]), (prec, vo, n)
             assert np.array_equal(q, ref[n][2]), (prec, vo, n)
+    # the pull-form variants (two lattices) after the 5 x 15 in-place ones
+    for v in range(5 * nv_even, nv):
+        for n in (3, 4):
+            f, u, q = debug_steps3d(solid, force, n, tau=0.8, precision=prec, variant=v)
+            assert np.array_equal(f, ref[n][0]) and np.array_equal(u, ref[n][1]), (prec, v, n)
+            assert np.array_equal(q, ref[n][2]), (prec, v, n)
 
 
 @pytest.mark.parametrize("prec,tol", [("fp32", 2e-6), ("fp16", 2e-3)])
