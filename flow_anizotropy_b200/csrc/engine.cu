@@ -173,12 +173,12 @@ int lbm_check_params3d(lbm_ctx *ctx, const lbm_params3d &p)
 
 // The autotuner's pick on the 128^3 tensor workload: FP32 the pull form
 // (voxel pairs, ranks from the neighbour record, 3 blocks per SM); 16-bit
-// bulk-staged odd + grouped even step with the link slots shared by the
-// directions and voxel pairs collided together.
+// the two-lattice AA form of the bulk-staged odd step + the grouped even
+// step with the link slots shared by the directions (4 blocks per SM).
 int lbm_default_variant(int prec)
 {
     if (prec == LBM_FP32) return NVAR_LP + 1;
-    if (prec == LBM_FP16 || prec == LBM_BF16) return 4 * NVAR_EVEN_LP + 11;
+    if (prec == LBM_FP16 || prec == LBM_BF16) return AA2_BASE_LP + 4 * NVAR_EVEN_LP + 9;
     return 0;
 }
 
@@ -208,19 +208,19 @@ long long lbm_lattice_bytes3d(long long n, int prec)
 }
 
 // Lattice bytes of one direction of a filled solve record (both lattices of
-// the pull form).
+// the pull and two-lattice AA forms).
 long long lbm_lattice_bytes(const Solve3 &S)
 {
     if (is_dense_m(S.prec)) return md_lattice_bytes(S.md);
-    return lbm_lattice_bytes3d(S.nfluid, S.prec) * (S.pull ? 2 : 1);
+    return lbm_lattice_bytes3d(S.nfluid, S.prec) * ((S.pull || S.aa2) ? 2 : 1);
 }
 
 // Point a solve record at its lattice memory (lbm_lattice_bytes(S) bytes);
-// the pull form's second lattice follows the first.
+// the second lattice of the two-lattice forms follows the first.
 void lbm_attach_lattice(Solve3 &S, void *p)
 {
     S.A = p;
-    S.B = S.pull ? static_cast<char *>(p) + lbm_lattice_bytes3d(S.nfluid, S.prec) : nullptr;
+    S.B = (S.pull || S.aa2) ? static_cast<char *>(p) + lbm_lattice_bytes3d(S.nfluid, S.prec) : nullptr;
 }
 
 // Plane stride (populations) or record slots per buffer (moments).
@@ -233,6 +233,8 @@ long long lbm_plane_for(int prec, long long n)
 int lbm_effective_variant(int prec, int variant, bool have_meta)
 {
     if (is_moment(prec) || is_dense_m(prec) || have_meta) return variant;
+    if (is_aa2_variant(prec, variant))
+        return aa2_base(prec) + lbm_effective_variant(prec, kernel_variant(prec, variant), false);
     if (is_pull_variant(prec, variant))
         return pull_meta(variant - NVAR_LP) ? NVAR_LP + 2 : variant;   // pull, ranks from the mask
     const int ve = variant % nvar_even(prec);
@@ -247,6 +249,7 @@ int lbm_effective_variant(int prec, int variant, bool have_meta)
 bool lbm_grouped_variant(int prec, int variant)
 {
     if (is_pull_variant(prec, variant)) return pull_grouped(variant - NVAR_LP);
+    variant = kernel_variant(prec, variant);
     return prec >= LBM_FP32 && prec <= LBM_BF16 && even_grouped(variant % NVAR_EVEN_LP);
 }
 
@@ -301,6 +304,7 @@ void lbm_fill_solve3(Solve3 &S, int nx, int ny, int nz, const double F[3], const
     memset(&S, 0, sizeof(S));
     S.prec = p.precision;
     S.pull = is_pull_variant(p.precision, p.variant) ? 1 : 0;
+    S.aa2 = is_aa2_variant(p.precision, p.variant) ? 1 : 0;
     S.nx = nx; S.ny = ny; S.nz = nz;
     S.wpr = (nx + 31) / 32;
     S.nn = (long long)nx * ny * nz;

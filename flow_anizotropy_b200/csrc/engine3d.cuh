@@ -134,6 +134,7 @@ struct Solve3 {
     MDGeom md;            // dense moment form only
     int group;            // grouped even step: directions in the group led by this record (else 0)
     int pull;             // two-lattice pull form (step3d_pull_kernel): A and B alternate
+    int aa2;              // two-lattice AA form: the even step scatters into the other lattice (aa_buf)
 };
 
 struct StepArgs {
@@ -155,6 +156,26 @@ struct StepArgs {
 // can matter again (every lag multiple, every phase end), so the step kernels
 // of a reduction step need no fence, ticket or last-tile pass.
 constexpr int DEFER_SLOTS = 64;
+
+// Lattice buffer m of a solve (A = 0, B = 1).  The in-place AA form uses A
+// for every step.  The two-lattice AA form (Solve3::aa2) runs step n with
+// source buffer ((n - 1) >> 1) & 1 and destination buffer (n >> 1) & 1: the
+// odd (local) step stays in place, and the even step gathers from one lattice
+// and scatters into the other, so no slot is read and rewritten in one
+// launch (the in-place even step's stores drop lines from the SM's L1 cache
+// that other warps' gathers still need; on the 128^3 workload's access
+// pattern alone, 119 -> 83 us per 2-byte launch and 152 -> 120 us per
+// 4-byte one).  The slots within a buffer are those of the in-place form, so
+// the kernels, their arithmetic and their bits are unchanged.
+template <class T>
+__device__ __forceinline__ T *aa_buf(const Solve3 &S, long long m)
+{
+    return static_cast<T *>((S.aa2 && (m & 1)) ? S.B : S.A);
+}
+template <class T>
+__device__ __forceinline__ T *aa_src(const Solve3 &S, long long n) { return aa_buf<T>(S, (n - 1) >> 1); }
+template <class T>
+__device__ __forceinline__ T *aa_dst(const Solve3 &S, long long n) { return aa_buf<T>(S, n >> 1); }
 
 // ----------------------------------------------------------------- helpers --
 __device__ __forceinline__ int mbit(const uint32_t *row, int x)
@@ -568,10 +589,21 @@ __host__ __device__ constexpr Variant even_f64(int v)
 // into shared memory (ranks from the record), 2 or 3 blocks per SM.  All but
 // 3 step a thread's two adjacent voxels together.
 constexpr int NVAR_PULL = 6;
-__host__ __device__ constexpr bool is_pull_variant(int prec, int v) { return prec >= 1 && prec <= 3 && v >= NVAR_LP; }
+__host__ __device__ constexpr bool is_pull_variant(int prec, int v)
+{
+    return prec >= 1 && prec <= 3 && v >= NVAR_LP && v < NVAR_LP + NVAR_PULL;
+}
 __host__ __device__ constexpr int pull_minb(int p) { return p == 3 ? 4 : (p == 0 || p == 2 || p == 4) ? 2 : 3; }
 __host__ __device__ constexpr bool pull_meta(int p) { return p != 2; }
 __host__ __device__ constexpr bool pull_grouped(int p) { return p >= 4; }
+// Two-lattice AA variants (Solve3::aa2) follow: the in-place variant v runs
+// as NVAR_LP + NVAR_PULL + v (FP32, FP16, BF16) or NVAR_F64 + v (FP64), the
+// same kernels with the even step scattering into the other lattice.
+constexpr int AA2_BASE_LP = NVAR_LP + NVAR_PULL;
+__host__ __device__ constexpr int aa2_base(int prec) { return prec == 0 ? NVAR_F64 : AA2_BASE_LP; }
+__host__ __device__ constexpr bool is_aa2_variant(int prec, int v) { return prec >= 0 && prec <= 3 && v >= aa2_base(prec); }
+// the in-place variant whose kernels a variant runs
+__host__ __device__ constexpr int kernel_variant(int prec, int v) { return is_aa2_variant(prec, v) ? v - aa2_base(prec) : v; }
 // pore voxels per tile: the odd and even kernels of one solve share the tile
 // list (and its partials), so both use TPB * TILE_NPT voxels per tile
 constexpr int TILE_NPT = 2;
@@ -645,7 +677,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_kernel(const StepArgs a)
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
         const bool red = step_reduces(a, S.c, phase, n);
-        T *__restrict__ A = static_cast<T *>(S.A);
+        T *__restrict__ A = aa_src<T>(S, n);          // odd steps run in place
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
@@ -744,7 +776,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_odd_pair_kernel(const StepAr
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
         const bool red = step_reduces(a, S.c, phase, n);
-        T *__restrict__ A = static_cast<T *>(S.A);
+        T *__restrict__ A = aa_src<T>(S, n);          // odd steps run in place
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
         const unsigned ts = (unsigned)item.y * (TPB * TILE_NPT);
@@ -869,15 +901,15 @@ __global__ void __launch_bounds__(ODD_BULK_THREADS, MINB) step3d_odd_bulk_kernel
                             const Solve3 &S = a.solves[it.x];
                             cx = it.x;
                             cphase = S.st->phase;
-                            c.A = S.A;
                             c.n = S.st->s_base + a.step + 1;
+                            c.A = aa_src<T>(S, c.n);          // odd steps run in place
                             c.P = (unsigned)S.plane;
                             c.nfluid = (unsigned)S.nfluid;
                             c.scale = S.scale;
                             c.inv_scale = S.inv_scale;
                             c.phys = S.P;
                             cred = cphase < PH_DONE && step_reduces(a, S.c, cphase, c.n) ? 1 : 0;
-                            if (cphase < PH_DONE && ((reinterpret_cast<uintptr_t>(S.A) | (uintptr_t)c.P * sizeof(T)) & 15u)) {
+                            if (cphase < PH_DONE && ((reinterpret_cast<uintptr_t>(c.A) | (uintptr_t)c.P * sizeof(T)) & 15u)) {
                                 // not a legal bulk copy (lattices are allocated
                                 // aligned and planes padded to 64 slots, so this
                                 // does not happen): the solve is failed instead
@@ -1017,7 +1049,8 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
         const bool red = step_reduces(a, S.c, phase, n);
-        T *__restrict__ A = static_cast<T *>(S.A);
+        const T *__restrict__ R = aa_src<T>(S, n);   // gathers
+        T *__restrict__ W = aa_dst<T>(S, n);         // scatters
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
         // the records of all of this thread's voxels are requested up front:
@@ -1047,21 +1080,21 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_kernel(const StepArgs a
                 compact_nbrs(S, i, x, y, z, nb);
             }
             Cp g[Q3];
-            g[0] = ST::ld(A + i);
+            g[0] = ST::ld(R + i);
 #pragma unroll
             for (int k = 1; k < Q3; ++k) {
                 const int o = opp3(k);
                 const unsigned src = ((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]);
-                g[k] = ST::ld(A + src);
+                g[k] = ST::ld(R + src);
             }
             Cp ux, uy, uz;
             collide3<ST, W1>(g, S, ux, uy, uz);
             const uint32_t hv = voxel_bits<ST>(i, n);
-            store_pop<ST>(A, i, g[0], hv, 0);
+            store_pop<ST>(W, i, g[0], hv, 0);
 #pragma unroll
             for (int k = 1; k < Q3; ++k) {
                 const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                store_pop<ST>(A, dst, g[k], hv, k);
+                store_pop<ST>(W, dst, g[k], hv, k);
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
@@ -1123,7 +1156,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_group_kernel(const Step
 #pragma unroll
             for (int d = 0; d < MAX_GROUP; ++d) {
                 if (!((live >> d) & 1u)) continue;
-                const T *__restrict__ A = static_cast<const T *>(a.solves[item.x + d].A);
+                const T *__restrict__ A = aa_src<const T>(a.solves[item.x + d], a.solves[item.x + d].st->s_base + a.step + 1);
                 g[d][0] = ST::ld(A + i);
 #pragma unroll
                 for (int k = 1; k < Q3; ++k) {
@@ -1136,7 +1169,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_group_kernel(const Step
             for (int d = 0; d < MAX_GROUP; ++d) {
                 if (!((live >> d) & 1u)) continue;
                 const Solve3 &S = a.solves[item.x + d];
-                T *__restrict__ A = static_cast<T *>(S.A);
+                T *__restrict__ A = aa_dst<T>(S, S.st->s_base + a.step + 1);
                 Cp ux, uy, uz;
                 collide3<ST, W1>(g[d], S, ux, uy, uz);
                 const uint32_t hv = voxel_bits<ST>(i, S.st->s_base + a.step + 1);
@@ -1225,32 +1258,33 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_links_kernel(const Step
             const Solve3 &S = a.solves[item.x + d];
             const long long n = S.st->s_base + a.step + 1;
             const bool red = step_reduces(a, S.c, S.st->phase, n);
-            T *__restrict__ A = static_cast<T *>(S.A);
+            const T *__restrict__ R = aa_src<T>(S, n);   // gathers
+            T *__restrict__ W = aa_dst<T>(S, n);         // scatters
             double acc[3] = {0.0, 0.0, 0.0};
             if constexpr (PAIR) {
                 const unsigned ia = i0 + tid, ib = i0 + TPB + tid;
                 const bool va = ia < nf, vb = ib < nf;
                 float2 g[Q3], u[3];
-                g[0].x = va ? ST::ld(A + ia) : 0.0f;
-                g[0].y = vb ? ST::ld(A + ib) : 0.0f;
+                g[0].x = va ? ST::ld(R + ia) : 0.0f;
+                g[0].y = vb ? ST::ld(R + ib) : 0.0f;
 #pragma unroll
                 for (int k = 1; k < Q3; ++k) {
-                    g[k].x = va ? ST::ld(A + sl[k - 1][tid]) : 0.0f;
-                    g[k].y = vb ? ST::ld(A + sl[k - 1][TPB + tid]) : 0.0f;
+                    g[k].x = va ? ST::ld(R + sl[k - 1][tid]) : 0.0f;
+                    g[k].y = vb ? ST::ld(R + sl[k - 1][TPB + tid]) : 0.0f;
                 }
                 collide3x2<ST, W1>(g, S, u);
                 if (va) {
                     const uint32_t hv = voxel_bits<ST>(ia, n);
-                    store_pop<ST>(A, ia, g[0].x, hv, 0);
+                    store_pop<ST>(W, ia, g[0].x, hv, 0);
 #pragma unroll
-                    for (int k = 1; k < Q3; ++k) store_pop<ST>(A, sl[opp3(k) - 1][tid], g[k].x, hv, k);
+                    for (int k = 1; k < Q3; ++k) store_pop<ST>(W, sl[opp3(k) - 1][tid], g[k].x, hv, k);
                     acc[0] += (double)u[0].x; acc[1] += (double)u[1].x; acc[2] += (double)u[2].x;
                 }
                 if (vb) {
                     const uint32_t hv = voxel_bits<ST>(ib, n);
-                    store_pop<ST>(A, ib, g[0].y, hv, 0);
+                    store_pop<ST>(W, ib, g[0].y, hv, 0);
 #pragma unroll
-                    for (int k = 1; k < Q3; ++k) store_pop<ST>(A, sl[opp3(k) - 1][TPB + tid], g[k].y, hv, k);
+                    for (int k = 1; k < Q3; ++k) store_pop<ST>(W, sl[opp3(k) - 1][TPB + tid], g[k].y, hv, k);
                     acc[0] += (double)u[0].y; acc[1] += (double)u[1].y; acc[2] += (double)u[2].y;
                 }
             } else {
@@ -1259,15 +1293,15 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_links_kernel(const Step
                     const unsigned i = i0 + j * TPB + tid;
                     if (i >= nf) continue;
                     Cp g[Q3];
-                    g[0] = ST::ld(A + i);
+                    g[0] = ST::ld(R + i);
 #pragma unroll
-                    for (int k = 1; k < Q3; ++k) g[k] = ST::ld(A + sl[k - 1][j * TPB + tid]);
+                    for (int k = 1; k < Q3; ++k) g[k] = ST::ld(R + sl[k - 1][j * TPB + tid]);
                     Cp ux, uy, uz;
                     collide3<ST, W1>(g, S, ux, uy, uz);
                     const uint32_t hv = voxel_bits<ST>(i, n);
-                    store_pop<ST>(A, i, g[0], hv, 0);
+                    store_pop<ST>(W, i, g[0], hv, 0);
 #pragma unroll
-                    for (int k = 1; k < Q3; ++k) store_pop<ST>(A, sl[opp3(k) - 1][j * TPB + tid], g[k], hv, k);
+                    for (int k = 1; k < Q3; ++k) store_pop<ST>(W, sl[opp3(k) - 1][j * TPB + tid], g[k], hv, k);
                     acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
                 }
             }
@@ -1331,18 +1365,19 @@ __global__ void __launch_bounds__(2 * TPB, MINB) step3d_even_links1_kernel(const
             const Solve3 &S = a.solves[item.x + d];
             const long long n = S.st->s_base + a.step + 1;
             const bool red = step_reduces(a, S.c, S.st->phase, n);
-            T *__restrict__ A = static_cast<T *>(S.A);
+            const T *__restrict__ R = aa_src<T>(S, n);   // gathers
+            T *__restrict__ W = aa_dst<T>(S, n);         // scatters
             Cp ux = Cp(0), uy = Cp(0), uz = Cp(0);
             if (v) {
                 Cp g[Q3];
-                g[0] = ST::ld(A + i);
+                g[0] = ST::ld(R + i);
 #pragma unroll
-                for (int k = 1; k < Q3; ++k) g[k] = ST::ld(A + sl[k - 1][tid]);
+                for (int k = 1; k < Q3; ++k) g[k] = ST::ld(R + sl[k - 1][tid]);
                 collide3<ST, W1>(g, S, ux, uy, uz);
                 const uint32_t hv = voxel_bits<ST>(i, n);
-                store_pop<ST>(A, i, g[0], hv, 0);
+                store_pop<ST>(W, i, g[0], hv, 0);
 #pragma unroll
-                for (int k = 1; k < Q3; ++k) store_pop<ST>(A, sl[opp3(k) - 1][tid], g[k], hv, k);
+                for (int k = 1; k < Q3; ++k) store_pop<ST>(W, sl[opp3(k) - 1][tid], g[k], hv, k);
             }
             if (red) {
                 su[0][tid] = (float)ux; su[1][tid] = (float)uy; su[2][tid] = (float)uz;
@@ -1384,7 +1419,8 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const Step
         if (phase >= PH_DONE) continue;
         const long long n = S.st->s_base + a.step + 1;
         const bool red = step_reduces(a, S.c, phase, n);
-        T *__restrict__ A = static_cast<T *>(S.A);
+        const T *__restrict__ R = aa_src<T>(S, n);   // gathers
+        T *__restrict__ W = aa_dst<T>(S, n);         // scatters
         const unsigned P = (unsigned)S.plane;
         double acc[3] = {0.0, 0.0, 0.0};
         uint4 mr[TILE_NPT];
@@ -1409,7 +1445,7 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const Step
                     const int o = opp3(k);
                     const unsigned src = k == 0 ? i : (((nb.solid >> o) & 1u) ? (k * P + i) : (o * P + nb.idx[o]));
                     par[j] |= (src & 1u) << k;
-                    __pipeline_memcpy_async(&stage[j][k][threadIdx.x], ST::word(A + src), sizeof(Wd));
+                    __pipeline_memcpy_async(&stage[j][k][threadIdx.x], ST::word(R + src), sizeof(Wd));
                 }
             }
             __pipeline_commit();
@@ -1427,11 +1463,11 @@ __global__ void __launch_bounds__(TPB, MINB) step3d_even_async_kernel(const Step
             CNb nb;
             meta_nbrs(S, i, mr[j], mr2[j], nb);
             const uint32_t hv = voxel_bits<ST>(i, n);
-            store_pop<ST>(A, i, g[0], hv, 0);
+            store_pop<ST>(W, i, g[0], hv, 0);
 #pragma unroll
             for (int k = 1; k < Q3; ++k) {
                 const unsigned dst = ((nb.solid >> k) & 1u) ? (opp3(k) * P + i) : (k * P + nb.idx[k]);
-                store_pop<ST>(A, dst, g[k], hv, k);
+                store_pop<ST>(W, dst, g[k], hv, k);
             }
             acc[0] += (double)ux; acc[1] += (double)uy; acc[2] += (double)uz;
         }
@@ -1717,8 +1753,10 @@ __global__ void canon3d_kernel(const Solve3 S, long long done, double *f_out, fl
         compact_nbrs(S, i, x, y, z, nb);
         double f[Q3];
         // pull form: the buffer step `done` wrote holds f*_k at [k][i] (the
-        // initial state, done = 0, sits in A)
-        const T *Ab = S.pull ? static_cast<const T *>((done & 1ll) ? S.B : S.A) : A;
+        // initial state, done = 0, sits in A); two-lattice AA form: the
+        // in-place slots, in the buffer step `done` wrote (aa_dst)
+        const T *Ab = S.pull ? static_cast<const T *>((done & 1ll) ? S.B : S.A)
+                    : S.aa2 ? aa_buf<const T>(S, done >> 1) : A;
 #pragma unroll
         for (int k = 0; k < Q3; ++k) {
             const int o = opp3(k);
@@ -1764,7 +1802,7 @@ inline bool is_dense_m(int prec) { return prec == 6; }
 // shared-memory ring depth x register budget.
 constexpr int NVAR_MD = 4;
 __host__ __device__ constexpr int md_lz(int v) { return v == 1 ? 32 : v == 2 ? 8 : 16; }
-inline int variant_count(int prec) { return prec == 0 ? NVAR_F64 : prec == 6 ? NVAR_MD : (prec >= 4 ? 3 : NVAR_LP + NVAR_PULL); }
+inline int variant_count(int prec) { return prec == 0 ? 2 * NVAR_F64 : prec == 6 ? NVAR_MD : (prec >= 4 ? 3 : AA2_BASE_LP + NVAR_LP); }
 // pore voxels per tile (in units of TPB) of a solve's tile list
 inline int variant_npt(int prec, int) { return prec >= 4 ? 1 : TILE_NPT; }
 

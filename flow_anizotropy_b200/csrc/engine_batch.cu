@@ -187,8 +187,9 @@ extern "C" long long lbm_batch_bytes3d(int nx, int ny, int nz, int ndir, int pre
         return tables + md_pmask_bytes(g, ny, nz) + (long long)ndir * (md_lattice_bytes(g) + 24ll * tiles);
     }
     const long long tiles = (nn + TPB - 1) / TPB;
-    // the pull form's two lattices, for the precisions that have it
-    const long long lat = lbm_lattice_bytes3d(nn, precision) * (is_pull_variant(precision, NVAR_LP) ? 2 : 1);
+    // the two lattices of the pull and two-lattice AA forms, for the
+    // precisions that have them
+    const long long lat = lbm_lattice_bytes3d(nn, precision) * (precision >= LBM_FP64 && precision <= LBM_BF16 ? 2 : 1);
     return tables + (long long)ndir * (lat + 8 * lbm_partial_doubles(precision, (int)tiles));
 }
 

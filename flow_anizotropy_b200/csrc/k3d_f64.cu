@@ -10,7 +10,8 @@ namespace lbm {
 
 cudaError_t launch_step3d_f64(int variant, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
-    if (variant < 0 || variant >= NVAR_F64) return cudaErrorInvalidValue;
+    if (variant < 0 || variant >= 2 * NVAR_F64) return cudaErrorInvalidValue;
+    variant = kernel_variant(0, variant);        // the two-lattice AA form runs the in-place kernels
     const int vo = variant / NVAR_EVEN, ve = variant % NVAR_EVEN;
     if (odd) {
         switch (vo) {
@@ -35,6 +36,7 @@ cudaError_t launch_step3d_f64(int variant, bool odd, dim3 grid, cudaStream_t s, 
 
 int max_blocks_f64(int variant, bool odd)
 {
+    variant = kernel_variant(0, variant);
     const int vo = variant / NVAR_EVEN, ve = variant % NVAR_EVEN;
     const void *k = odd ? (vo == 0 ? (const void *)LBM_ODD(0) : vo == 1 ? (const void *)LBM_ODD(1) : (const void *)LBM_ODD(2))
                         : (ve == 0 ? (const void *)LBM_EVEN(0) : ve == 1 ? (const void *)LBM_EVEN(1)

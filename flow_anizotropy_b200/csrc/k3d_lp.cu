@@ -126,6 +126,7 @@ static cudaError_t launch_lp(int v, bool odd, dim3 grid, cudaStream_t s, const S
 
 cudaError_t launch_step3d_lp(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const StepArgs &a)
 {
+    variant = kernel_variant(prec, variant);     // the two-lattice AA form runs the in-place kernels
     switch (prec) {
     case 1: return w1 ? launch_lp<StoreF32, true>(variant, odd, grid, s, a) : launch_lp<StoreF32, false>(variant, odd, grid, s, a);
     case 2: return w1 ? launch_lp<StoreF16, true>(variant, odd, grid, s, a) : launch_lp<StoreF16, false>(variant, odd, grid, s, a);
@@ -165,6 +166,7 @@ static int occ(int v, bool odd)
 
 int max_blocks_step3d(int prec, int variant, bool odd)
 {
+    variant = kernel_variant(prec, variant);
     switch (prec) {
     case 0: return max_blocks_f64(variant, odd);
     case 1: return occ<StoreF32>(variant, odd);

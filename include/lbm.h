@@ -43,12 +43,15 @@ extern "C" {
 
 /* lbm_params3d.variant: the library's default for the precision (the
  * variant the autotuner picks on the 128^3 tensor workload: FP32 76, FP16 and
- * BF16 71, 0 otherwise; a batch, which steps each direction on its own,
+ * BF16 150, 0 otherwise; a batch, which steps each direction on its own,
  * defaults to FP16 and BF16 61).  Every variant of a precision gives the same
  * bits.  For FP32, FP16 and BF16, variants v < 75 are the in-place (AA)
  * lattice, odd-step kernel v / 15 and even-step kernel v % 15; v = 75..80
- * are the two-lattice pull form (one kernel for every step, twice the
- * lattice memory).  FP64: odd-step kernel v / 6 and even-step kernel v % 6. */
+ * are the two-lattice pull form (one kernel for every step); v = 81..155 are
+ * the two-lattice AA form of in-place variant v - 81 (the same kernels, the
+ * even step scattering into the other lattice).  FP64: odd-step kernel v / 6
+ * and even-step kernel v % 6 for v < 18, the two-lattice AA form of v - 18
+ * for v = 18..35.  The two-lattice forms take twice the lattice memory. */
 #define LBM_VARIANT_DEFAULT (-1)
 
 /* Population storage (collision arithmetic is FP64 for LBM_FP64, else FP32;

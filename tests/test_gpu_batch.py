@@ -105,8 +105,9 @@ def test_batch_variant_choice(gpu):
     nve = 15                                    # even variants per odd variant
     pair_meta = 3 * nve + 1                     # odd: voxel pairs; even: neighbour records
     pull = 5 * nve                              # the two-lattice pull form, per direction
+    aa2 = pull + 6                              # the two-lattice AA form of in-place variant v: aa2 + v
     out = {}
-    for v in (-1, 1, pair_meta, pull, pull + 3):
+    for v in (-1, 1, pair_meta, pull, pull + 3, aa2 + 4 * nve + 1):
         b = S.Batch(precision="fp16", hbm_budget=4 * 2**30, chunk=32, variant=v)
         for t, s in enumerate(structs):
             assert b.submit(s, _forces(), p, tag=t)
@@ -121,7 +122,7 @@ def test_batch_variant_choice(gpu):
                 break
         out[v] = done
         b.close()
-    for v in (1, pair_meta, pull, pull + 3):
+    for v in (1, pair_meta, pull, pull + 3, aa2 + 4 * nve + 1):
         for t in range(len(structs)):
             for a, m in zip(out[-1][t], out[v][t]):
                 assert a.steps == m.steps and np.array_equal(a.q, m.q) and np.array_equal(a.se, m.se), v
@@ -134,4 +135,6 @@ def test_batch_variant_choice(gpu):
         b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, 6))
     with pytest.raises(_lib.LBMError, match="grouped"):
         b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, pull + 4))
+    with pytest.raises(_lib.LBMError, match="grouped"):
+        b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, aa2 + 6))
     b.close()

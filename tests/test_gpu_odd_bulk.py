@@ -74,7 +74,7 @@ def test_bulk_odd_whole_solves_identical(gpu, prec):
 
 def test_variant_table_has_bulk_odd(gpu):
     for prec in ("fp32", "fp16", "bf16"):
-        assert S.variant_count(prec) == 5 * NV_EVEN + 6      # + the pull-form variants
+        assert S.variant_count(prec) == 5 * NV_EVEN + 6 + 5 * NV_EVEN   # + pull form + two-lattice AA form
 
 
 def test_starved_waits_end_with_status(gpu):
@@ -100,7 +100,8 @@ def test_starved_waits_end_with_status(gpu):
     assert rc == rc0 and ok[0].steps == ref[0].steps and np.array_equal(ok[0].q, ref[0].q)
 
 
-@pytest.mark.parametrize("prec,default", [("fp32", 5 * NV_EVEN + 1), ("fp16", 4 * NV_EVEN + 11), ("bf16", 4 * NV_EVEN + 11),
+@pytest.mark.parametrize("prec,default", [("fp32", 5 * NV_EVEN + 1), ("fp16", 5 * NV_EVEN + 6 + 4 * NV_EVEN + 9),
+                                          ("bf16", 5 * NV_EVEN + 6 + 4 * NV_EVEN + 9),
                                           ("fp64", 0)])
 def test_default_variant_is_the_tuned_pick_and_matches_variant_0(gpu, prec, default):
     """LBM_VARIANT_DEFAULT runs the listed variant; since every variant sums

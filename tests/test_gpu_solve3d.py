@@ -35,6 +35,20 @@ def test_fp64_matches_oracle(gpu, packing, oracle_runs):
         assert np.abs(g.se - r["se"]).max() <= 1e-8 * scale
 
 
+def test_fp64_two_lattice_aa(gpu, packing, oracle_runs):
+    """FP64 in the two-lattice AA form (variants 18-35: the in-place kernels
+    with the even step scattering into the other lattice) takes the oracle's
+    step counts, bit for bit with the in-place form."""
+    forces, ref = oracle_runs
+    a, _, _ = S.solve3d(packing, forces, S.Params3D(precision="fp64", variant=0, **PRM))
+    assert S.variant_count("fp64") == 36
+    for v in (18, 18 + 2, 18 + 13):
+        b, _, _ = S.solve3d(packing, forces, S.Params3D(precision="fp64", variant=v, **PRM))
+        for x, y, r in zip(a, b, ref):
+            assert x.steps == y.steps == r["steps"], v
+            assert np.array_equal(x.q, y.q) and np.array_equal(x.se, y.se), v
+
+
 @pytest.mark.parametrize("prec,tol,crit", [("fp32", 1e-4, "auto"), ("fp16", 1e-3, "auto"), ("bf16", 1e-3, "auto"),
                                            ("fp16", 1e-3, "block"), ("fp32", 1e-4, "batch")])
 def test_reduced_precision(gpu, packing, oracle_runs, prec, tol, crit):
@@ -92,27 +106,30 @@ def test_grouped_even_step_equals_per_direction(gpu, packing, prec, ndir):
             assert a.steps == b.steps and a.converged == b.converged
             assert np.array_equal(a.q, b.q) and np.array_equal(a.se, b.se), ve
         assert np.array_equal(vel, vel0), ve
-    assert S.variant_count(prec) == 5 * nv_even + NV_PULL
+    assert S.variant_count(prec) == 5 * nv_even + NV_PULL + 5 * nv_even
 
 
 NV_PULL = 6          # pull-form variants after the 5 x 15 in-place ones
+AA2 = 5 * 15 + NV_PULL   # then the two-lattice AA form of every in-place variant
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp16", "bf16"])
 @pytest.mark.parametrize("ndir", [3, 4, 1])
 def test_pull_form_equals_in_place(gpu, packing, prec, ndir):
-    """The two-lattice pull form (one kernel for every step, gathers from the
-    other lattice, coalesced stores to its own) gives the in-place AA
-    kernels' bits over whole solves: step counts, fluxes, standard errors and
-    the exported velocity field, for every pull variant (per direction, one
-    voxel per thread, grouped), also with a group of one after a group of
-    three."""
+    """The two-lattice forms give the in-place AA kernels' bits over whole
+    solves (step counts, fluxes, standard errors and the exported velocity
+    field), also with a group of one after a group of three: the pull form
+    (one kernel for every step, gathers from the other lattice, coalesced
+    stores to its own), every pull variant; and the two-lattice AA form (the
+    in-place kernels with the even step scattering into the other lattice)."""
     F = 1e-6
     forces = [[F, 0, 0], [0, F, 0], [0, 0, F], [F / 3**0.5] * 3][:ndir]
     base = 5 * 15
     ref, rc0, vel0 = S.solve3d(packing, forces, S.Params3D(precision=prec, variant=1, **PRM), velocity=True)
     assert ref[0].steps > 0
-    for q in range(NV_PULL):
+    # the pull variants, then the two-lattice AA form of the per-direction,
+    # grouped, link-slot and bulk-staged in-place variants
+    for q in list(range(NV_PULL)) + [AA2 - base + v for v in (1, 3, 7, 11, 14, 61, 69, 71, 74)]:
         got, rc, vel = S.solve3d(packing, forces, S.Params3D(precision=prec, variant=base + q, **PRM), velocity=True)
         assert rc == rc0
         for a, b in zip(ref, got):
@@ -128,7 +145,7 @@ def test_pull_form_general_tau(gpu, packing):
     forces = [[0, F, 0], [0, 0, F]]
     prm = dict(PRM, max_steps=1500)
     ref, rc0, _ = S.solve3d(packing, forces, S.Params3D(precision="fp16", tau=0.8, variant=1, **prm))
-    for q in (0, 3, 4):
+    for q in (0, 3, 4, AA2 - 75 + 71, AA2 - 75 + 1):
         got, rc, _ = S.solve3d(packing, forces, S.Params3D(precision="fp16", tau=0.8, variant=75 + q, **prm))
         for a, b in zip(ref, got):
             assert a.steps == b.steps and np.array_equal(a.q, b.q) and np.array_equal(a.se, b.se), q

@@ -105,13 +105,15 @@ def test_every_odd_variant_agrees_general_tau(gpu, prec):
     nv = _lib.load().lbm_variant_count(_lib.PRECISIONS[prec])
     nv_even = 15      # NVAR_EVEN_LP
     ref = {n: debug_steps3d(solid, force, n, tau=0.8, precision=prec, variant=1) for n in (3, 4)}
-    for vo in range(1, nv // nv_even):
+    assert nv == 5 * nv_even + 6 + 5 * nv_even
+    for vo in range(1, 5):
         for n in (3, 4):
             f, u, q = debug_steps3d(solid, force, n, tau=0.8, precision=prec, variant=vo * nv_even + 1)
             assert np.array_equal(f, ref[n][0]) and np.array_equal(u, ref[n][1]), (prec, vo, n)
             assert np.array_equal(q, ref[n][2]), (prec, vo, n)
-    # the pull-form variants (two lattices) after the 5 x 15 in-place ones
-    for v in range(5 * nv_even, nv):
+    # the pull-form variants (two lattices) after the 5 x 15 in-place ones,
+    # then the two-lattice AA form of each odd variant with the same even one
+    for v in list(range(5 * nv_even, 5 * nv_even + 6)) + [5 * nv_even + 6 + vo * nv_even + 1 for vo in range(5)]:
         for n in (3, 4):
             f, u, q = debug_steps3d(solid, force, n, tau=0.8, precision=prec, variant=v)
             assert np.array_equal(f, ref[n][0]) and np.array_equal(u, ref[n][1]), (prec, v, n)
