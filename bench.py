@@ -191,16 +191,20 @@ TRAFFIC = ROOT / "profiles" / "traffic.json"
 
 def profiled_traffic(prec, variant, updates_per_launch):
     """DRAM bytes (read + write) per step launch of this run's step kernels,
-    from the ncu capture recorded in profiles/traffic.json (per pore-voxel
-    update, the mean of one odd and one even launch, with the command that
-    measured it), scaled to this run's updates per launch.  None when no
-    capture of this precision and kernel variant is recorded."""
+    from the ncu captures recorded in profiles/traffic.json (per precision, a
+    list of kernel variants, each per pore-voxel update: the mean of one odd
+    and one even launch, with the command that measured it), scaled to this
+    run's updates per launch.  None when no capture of this precision and
+    kernel variant is recorded."""
     if not TRAFFIC.exists():
         return None
-    rec = json.loads(TRAFFIC.read_text()).get(prec)
-    if not rec or rec.get("variant") != variant:
-        return None
-    return rec["dram_bytes_per_update"] * updates_per_launch
+    recs = json.loads(TRAFFIC.read_text()).get(prec) or []
+    if isinstance(recs, dict):
+        recs = [recs]
+    for rec in recs:
+        if rec.get("variant") == variant:
+            return rec["dram_bytes_per_update"] * updates_per_launch
+    return None
 
 
 def tensor_K(runs, mu, F):

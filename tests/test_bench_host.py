@@ -28,6 +28,12 @@ def test_profiled_traffic_scaled_from_the_recorded_capture(tmp_path, monkeypatch
     assert bench.profiled_traffic("fp16", 7, 1000.0) == 70_000.0
     assert bench.profiled_traffic("fp16", 8, 1000.0) is None        # another kernel variant: not this capture
     assert bench.profiled_traffic("fp32", 7, 1000.0) is None
+    # several captured variants of one precision
+    f.write_text(__import__("json").dumps({"bf16": [{"variant": 150, "dram_bytes_per_update": 61.0},
+                                                    {"variant": 71, "dram_bytes_per_update": 60.0}]}))
+    assert bench.profiled_traffic("bf16", 71, 10.0) == 600.0
+    assert bench.profiled_traffic("bf16", 150, 10.0) == 610.0
+    assert bench.profiled_traffic("bf16", 69, 10.0) is None
     monkeypatch.setattr(bench, "TRAFFIC", tmp_path / "absent.json")
     assert bench.profiled_traffic("fp16", 7, 1000.0) is None
 
@@ -38,9 +44,13 @@ def test_recorded_traffic_within_the_algorithmic_bytes():
     import json
     if not bench.TRAFFIC.exists():
         return
-    for prec, rec in json.loads(bench.TRAFFIC.read_text()).items():
+    for prec, recs in json.loads(bench.TRAFFIC.read_text()).items():
+        if prec.startswith("_"):
+            continue
         alg = bench.BYTES_PER_UPDATE[prec] + 1.0 / 8 / 0.45
-        assert 0 < rec["dram_bytes_per_update"] <= 1.05 * alg, (prec, rec)
+        for rec in (recs if isinstance(recs, list) else [recs]):
+            assert 0 < rec["dram_bytes_per_update"] <= 1.05 * alg, (prec, rec)
+            assert "ncu" in rec["command"]
 
 
 def test_reference_row_of_the_workload():
