@@ -182,11 +182,10 @@ int lbm_default_variant(int prec)
     return 0;
 }
 
-// The batch steps each direction on its own (no grouped even kernels): its
-// default is the best per-direction pick, even step from neighbour records.
+// The batch's default: the solve default (its 16-bit pick has a grouped even
+// step, which the batch runs over runs of a structure's consecutive slots).
 int lbm_default_batch_variant(int prec)
 {
-    if (prec == LBM_FP16 || prec == LBM_BF16) return 4 * NVAR_EVEN_LP + 1;
     return lbm_default_variant(prec);
 }
 
@@ -254,7 +253,7 @@ bool lbm_grouped_variant(int prec, int variant)
 }
 
 // Do all launches (not only the even ones) of this variant take the grouped work list?
-static bool lbm_grouped_all(int prec, int variant)
+bool lbm_grouped_all(int prec, int variant)
 {
     return is_pull_variant(prec, variant) && pull_grouped(variant - NVAR_LP);
 }

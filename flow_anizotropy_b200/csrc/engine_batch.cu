@@ -37,6 +37,7 @@ struct Slot {
     DevMem partials{nullptr};
     long long bytes = 0;
     long long tables = 0;     // mask + rank tables of the structure
+    int lead = -1;            // grouped variants: first slot of this direction's group
 };
 
 }  // namespace
@@ -54,6 +55,11 @@ struct lbm_batch {
     int cap_work = 0;
     int nwork = 0;         // items in the device work list (= blocks per step launch)
     int graph_nwork = -1;  // launch size the graph holds
+    // grouped even-step variants: the even launches take a second work list of
+    // (group leader slot, tile) items; a group's slots are consecutive
+    bool grouped = false;
+    int ngwork = 0, graph_ngwork = -1, cap_gwork = 0;
+    DevMem d_gwork{nullptr}, d_ngwork{nullptr};
     int slot_hi = 0;       // slots below this index hold every resident solve
     int graph_slot_hi = -1;
     DevMem d_qbuf{nullptr};   // deferred reduction: q and flag per slot and step
@@ -86,6 +92,13 @@ static int capture(lbm_batch *b)
     const dim3 grid(std::max(1, b->nwork));
     const bool defer = lbm_defers(b->precision);
     a.defer = defer ? 2 : 0;
+    StepArgs ae = a;                 // even launches: the grouped work list when grouped
+    dim3 grid_e = grid;
+    if (b->grouped) {
+        ae.work = static_cast<const int2 *>(b->d_gwork.p);
+        ae.nwork_dev = static_cast<const int *>(b->d_ngwork.p);
+        grid_e = dim3(std::max(1, b->ngwork));
+    }
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     // chunks are even and solves join at chunk boundaries (s_base even), so
@@ -95,8 +108,9 @@ static int capture(lbm_batch *b)
     // change inside a pass (mode 2)
     for (int i = 0; i < b->chunk && e == cudaSuccess; ++i) {
         a.step = i;
+        ae.step = i;
         const bool odd = ((i + 1) & 1) == 1;
-        e = lbm_launch_step(b->precision, b->variant, b->w1, odd, grid, ctx->stream, a);
+        e = lbm_launch_step(b->precision, b->variant, b->w1, odd, odd ? grid : grid_e, ctx->stream, odd ? a : ae);
         const bool pass_end = ((i + 1) % DEFER_SLOTS) == 0 || i + 1 == b->chunk;
         if (e == cudaSuccess && defer && pass_end) {
             const int first = i - (i % DEFER_SLOTS);
@@ -119,6 +133,7 @@ static int capture(lbm_batch *b)
             if (b->graph) cudaGraphDestroy(b->graph);
             b->graph = g;
             b->graph_nwork = b->nwork;
+            b->graph_ngwork = b->ngwork;
             b->graph_slot_hi = b->slot_hi;
             return LBM_OK;
         }
@@ -128,6 +143,7 @@ static int capture(lbm_batch *b)
     b->graph = g;
     CK(cudaGraphInstantiate(&b->exec, g, 0));
     b->graph_nwork = b->nwork;
+    b->graph_ngwork = b->ngwork;
     b->graph_slot_hi = b->slot_hi;
     return LBM_OK;
 }
@@ -154,14 +170,32 @@ static int sync_work(lbm_batch *b)
         if (!s.retired)
             for (int t = 0; t < s.S.ntiles; ++t) work.push_back(make_int2(i, t));
     }
-    const int nwork = (int)work.size();
-    bool recapture = nwork != b->graph_nwork || b->slot_hi != b->graph_slot_hi;
+    // grouped even steps: one item per tile of every group with a direction
+    // still running (its slots stay resident until the whole group is done)
+    std::vector<int2> gwork;
+    if (b->grouped)
+        for (int i = 0; i < b->cap_slots; ++i) {
+            const Slot &s = b->slots[i];
+            if (!s.used || s.lead != i) continue;
+            bool live = false;
+            for (int d = 0; d < s.S.group; ++d) live = live || !b->slots[i + d].retired;
+            if (live)
+                for (int t = 0; t < s.S.ntiles; ++t) gwork.push_back(make_int2(i, t));
+        }
+    const int nwork = (int)work.size(), ngwork = (int)gwork.size();
+    bool recapture = nwork != b->graph_nwork || b->slot_hi != b->graph_slot_hi || ngwork != b->graph_ngwork;
     if (nwork > b->cap_work) {
         b->cap_work = std::max<int>(nwork, 2 * b->cap_work);
         CK(b->d_work.alloc(sizeof(int2) * (size_t)b->cap_work));
         recapture = true;
     }
+    if (ngwork > b->cap_gwork) {
+        b->cap_gwork = std::max<int>(ngwork, 2 * b->cap_gwork);
+        CK(b->d_gwork.alloc(sizeof(int2) * (size_t)b->cap_gwork));
+        recapture = true;
+    }
     b->nwork = nwork;
+    b->ngwork = ngwork;
     if (recapture) {
         int rc = capture(b);
         if (rc) return rc;
@@ -169,6 +203,9 @@ static int sync_work(lbm_batch *b)
     CK(cudaMemcpyAsync(b->d_solves.p, desc.data(), sizeof(Solve3) * b->cap_slots, cudaMemcpyHostToDevice, ctx->stream));
     if (nwork)
         CK(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, ctx->stream));
+    if (ngwork)
+        CK(cudaMemcpyAsync(b->d_gwork.p, gwork.data(), sizeof(int2) * gwork.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b->d_ngwork.p, &ngwork, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     // pageable source: the copy is staged before the call returns
     CK(cudaMemcpyAsync(b->d_nwork.p, &nwork, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -222,6 +259,12 @@ extern "C" int lbm_batch_create(lbm_ctx *ctx, lbm_batch **out, int precision, lo
     CK(b->d_states.alloc(sizeof(State3) * b->cap_slots));
     CK(b->d_work.alloc(sizeof(int2) * b->cap_work));
     CK(b->d_nwork.alloc(sizeof(int)));
+    b->d_gwork = DevMem(ctx->stream);
+    b->d_ngwork = DevMem(ctx->stream);
+    b->cap_gwork = 1 << 14;
+    CK(b->d_gwork.alloc(sizeof(int2) * b->cap_gwork));
+    CK(b->d_ngwork.alloc(sizeof(int)));
+    b->grouped = lbm_grouped_variant(precision, b->variant);
     b->d_qbuf = DevMem(ctx->stream);
     CK(b->d_qbuf.alloc(sizeof(double) * 4 * DEFER_SLOTS * (size_t)b->cap_slots));
     std::vector<State3> done(b->cap_slots);
@@ -243,11 +286,13 @@ extern "C" int lbm_batch_set_variant(lbm_batch *b, int variant)
     for (const Slot &s : b->slots)
         if (s.used) return lbm_fail_input(ctx, "the batch has resident solves");
     if (variant_npt(b->precision, variant) != b->npt) return lbm_fail_input(ctx, "variant changes the tile size");
-    if (lbm_grouped_variant(b->precision, variant))
-        return lbm_fail_input(ctx, "grouped even-step variants need a structure's directions in one work item; "
-                                   "the batch steps each direction on its own");
+    if (lbm_grouped_all(b->precision, variant))
+        return lbm_fail_input(ctx, "grouped pull variants step every launch by structure; the batch steps its "
+                                   "odd launches per direction");
     b->variant = variant;
+    b->grouped = lbm_grouped_variant(b->precision, variant);
     b->graph_nwork = -1;      // recapture with the new kernels at the next change
+    b->graph_ngwork = -1;
     return LBM_OK;
 }
 
@@ -277,8 +322,20 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
     int rc = lbm_check_params3d(ctx, p);
     if (rc) return rc;
     std::vector<int> free_slots;
-    for (int i = 0; i < b->cap_slots && (int)free_slots.size() < ndir; ++i)
-        if (!b->slots[i].used) free_slots.push_back(i);
+    if (b->grouped) {
+        // a structure's directions take consecutive slots (one group of up
+        // to MAX_GROUP per run), so the grouped even kernel finds them at
+        // leader + d
+        for (int i = 0; i + ndir <= b->cap_slots && (int)free_slots.size() < ndir; ++i) {
+            int run = 0;
+            while (run < ndir && !b->slots[i + run].used) ++run;
+            if (run == ndir) for (int d = 0; d < ndir; ++d) free_slots.push_back(i + d);
+            else i += run;
+        }
+    } else {
+        for (int i = 0; i < b->cap_slots && (int)free_slots.size() < ndir; ++i)
+            if (!b->slots[i].used) free_slots.push_back(i);
+    }
     if ((int)free_slots.size() < ndir) { ctx->err = "batch slots exhausted"; return LBM_EBUSY; }
 
     auto mask = std::make_shared<DevMem>(ctx->stream);
@@ -294,7 +351,10 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
     if (rc) return rc;
     if (!proto.meta && lbm_effective_variant(b->precision, b->variant, false) != b->variant) {
         // a structure too wide for neighbour records: the batch computes ranks
+        // (the mask-rank counterpart of a grouped variant is grouped too, so
+        // the resident groups keep their layout)
         b->variant = lbm_effective_variant(b->precision, b->variant, false);
+        b->grouped = lbm_grouped_variant(b->precision, b->variant);
         rc = capture(b);
         if (rc) return rc;
     }
@@ -318,6 +378,10 @@ extern "C" int lbm_batch_submit3d(lbm_batch *b, const uint8_t *solid, int nx, in
         Slot &s = b->slots[free_slots[j]];
         lbm_fill_solve3(s.S, nx, ny, nz, forces + 3 * j, p, b->npt);
         lbm_copy_pores(s.S, proto);
+        // group leader of direction j: the first of its run of MAX_GROUP
+        const int j0 = j - j % MAX_GROUP;
+        s.lead = b->grouped ? free_slots[j0] : -1;
+        if (b->grouped && j == j0) s.S.group = std::min(MAX_GROUP, ndir - j0);
         s.wpre = wpre; s.fnode = fnode; s.meta = meta; s.meta2 = meta2;
         s.tables = tables;
         CK(s.lattice.alloc((size_t)lbm_lattice_bytes(s.S)));
@@ -349,6 +413,25 @@ extern "C" int lbm_batch_run(lbm_batch *b, int chunks)
     return LBM_OK;
 }
 
+// Free a finished solve's slot: its lattice, partials and, with the
+// structure's last direction, the mask and rank tables.
+static void release_slot(lbm_batch *b, Slot &s)
+{
+    s.used = false;
+    s.lead = -1;
+    s.lattice.release();
+    s.partials.release();
+    b->resident -= s.bytes;
+    // the structure's mask goes with its last direction
+    const bool last = s.mask.use_count() == 1;
+    if (last) b->resident -= s.tables;
+    s.mask.reset();
+    s.wpre.reset();
+    s.fnode.reset();
+    s.meta.reset();
+    s.meta2.reset();
+}
+
 extern "C" int lbm_batch_poll(lbm_batch *b, long long *tags, int *dirs, lbm_result3d *results, int max, int *n)
 {
     if (!b || !n) return LBM_EINPUT;
@@ -372,19 +455,18 @@ extern "C" int lbm_batch_poll(lbm_batch *b, long long *tags, int *dirs, lbm_resu
         dirs[*n] = s.dir;
         ++*n;
         s.retired = true;
-        s.used = false;
-        s.lattice.release();
-        s.partials.release();
-        b->resident -= s.bytes;
-        // the structure's mask goes with its last direction
-        const bool last = s.mask.use_count() == 1;
-        if (last) b->resident -= s.tables;
-        s.mask.reset();
-        s.wpre.reset();
-        s.fnode.reset();
-        s.meta.reset();
-        s.meta2.reset();
         changed = true;
+        if (s.lead < 0) {
+            release_slot(b, s);
+            continue;
+        }
+        // grouped: the group's slots stay resident (the grouped even kernel
+        // reads its leader's record) until every direction of it is done
+        const int lead = s.lead, ng = b->slots[lead].S.group;
+        bool all = true;
+        for (int d = 0; d < ng; ++d) all = all && b->slots[lead + d].retired;
+        if (all)
+            for (int d = 0; d < ng; ++d) release_slot(b, b->slots[lead + d]);
     }
     if (changed) return sync_work(b);
     return LBM_OK;

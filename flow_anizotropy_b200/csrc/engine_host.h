@@ -79,6 +79,8 @@ int lbm_build_pores(lbm_ctx *ctx, lbm::Solve3 &S, int npt, DevMem &wpre, DevMem 
 int lbm_effective_variant(int prec, int variant, bool have_meta);
 // Does the variant step a structure's directions in one work item (grouped work list)?
 bool lbm_grouped_variant(int prec, int variant);
+// ... and do all of its launches (the grouped pull form)?
+bool lbm_grouped_all(int prec, int variant);
 void lbm_attach_lattice(lbm::Solve3 &S, void *p);
 void lbm_copy_pores(lbm::Solve3 &dst, const lbm::Solve3 &src);
 cudaError_t lbm_launch_step(int prec, int variant, bool w1, bool odd, dim3 grid, cudaStream_t s, const lbm::StepArgs &a);

@@ -43,8 +43,8 @@ extern "C" {
 
 /* lbm_params3d.variant: the library's default for the precision (the
  * variant the autotuner picks on the 128^3 tensor workload: FP32 76, FP16 and
- * BF16 150, 0 otherwise; a batch, which steps each direction on its own,
- * defaults to FP16 and BF16 61).  Every variant of a precision gives the same
+ * BF16 150, 0 otherwise; a batch takes the same defaults).  Every variant of
+ * a precision gives the same
  * bits.  For FP32, FP16 and BF16, variants v < 75 are the in-place (AA)
  * lattice, odd-step kernel v / 15 and even-step kernel v % 15; v = 75..80
  * are the two-lattice pull form (one kernel for every step); v = 81..155 are
@@ -208,11 +208,13 @@ int  lbm_batch_create(lbm_ctx *ctx, lbm_batch **batch, int precision,
                       long long hbm_budget, int chunk);
 
 /* Step-kernel variant of every launch of an empty batch (default
- * LBM_VARIANT_DEFAULT, the best per-direction variant lbm_tune3d finds on the
- * 128^3 tensor workload; mixes of small structures may prefer another).  Results do not
- * depend on it.  LBM_EINPUT while solves are resident, and for the grouped
- * even-step variants (they step all directions of a structure in one work
- * item; the batch steps each direction on its own). */
+ * LBM_VARIANT_DEFAULT, the variant lbm_tune3d picks on the 128^3 tensor
+ * workload; mixes of small structures may prefer another).  Results do not
+ * depend on it.  With a grouped even-step variant a structure's directions
+ * take consecutive slots and stay resident until all of them are done.
+ * LBM_EINPUT while solves are resident, and for the grouped pull variants
+ * (79-80: every launch by structure; the batch steps its odd launches per
+ * direction). */
 int  lbm_batch_set_variant(lbm_batch *batch, int variant);
 void lbm_batch_destroy(lbm_batch *batch);
 

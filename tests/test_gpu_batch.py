@@ -107,7 +107,9 @@ def test_batch_variant_choice(gpu):
     pull = 5 * nve                              # the two-lattice pull form, per direction
     aa2 = pull + 6                              # the two-lattice AA form of in-place variant v: aa2 + v
     out = {}
-    for v in (-1, 1, pair_meta, pull, pull + 3, aa2 + 4 * nve + 1):
+    # per direction (1, voxel pairs, pull forms, two-lattice AA) and grouped
+    # even steps (6, 71 in place; -1 is the default 150, two-lattice AA)
+    for v in (-1, 1, pair_meta, pull, pull + 3, aa2 + 4 * nve + 1, 6, 4 * nve + 11):
         b = S.Batch(precision="fp16", hbm_budget=4 * 2**30, chunk=32, variant=v)
         for t, s in enumerate(structs):
             assert b.submit(s, _forces(), p, tag=t)
@@ -122,19 +124,50 @@ def test_batch_variant_choice(gpu):
                 break
         out[v] = done
         b.close()
-    for v in (1, pair_meta, pull, pull + 3, aa2 + 4 * nve + 1):
+    for v in (1, pair_meta, pull, pull + 3, aa2 + 4 * nve + 1, 6, 4 * nve + 11):
         for t in range(len(structs)):
             for a, m in zip(out[-1][t], out[v][t]):
                 assert a.steps == m.steps and np.array_equal(a.q, m.q) and np.array_equal(a.se, m.se), v
     b = S.Batch(precision="fp16", hbm_budget=4 * 2**30, chunk=32)
     with pytest.raises(_lib.LBMError):
         b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, 10**6))
-    # grouped even-step variants step all directions of a structure in one
-    # work item; the batch steps each direction on its own and refuses them
-    with pytest.raises(_lib.LBMError, match="grouped"):
-        b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, 6))
+    # the grouped pull variants step every launch by structure; the batch
+    # steps its odd launches per direction and refuses them
     with pytest.raises(_lib.LBMError, match="grouped"):
         b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, pull + 4))
     with pytest.raises(_lib.LBMError, match="grouped"):
-        b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, aa2 + 6))
+        b.ctx.check(b.ctx.L.lbm_batch_set_variant(b.h, pull + 5))
     b.close()
+
+
+@pytest.mark.parametrize("prec", ["fp16", "fp32"])
+def test_grouped_batch_slots_and_reuse(gpu, prec):
+    """A grouped even-step variant in a batch (the 16-bit default; in-place
+    variant 71 for FP32): structures of 4, 1 and 3 directions (groups of
+    3 + 1, 1 and 3), directions finishing at different steps, a budget that
+    makes later structures wait for a whole group to leave and reuse its
+    slots: every result equals the solve alone bit for bit."""
+    structs = _mix()
+    F = 1e-6
+    fsets = [_forces(F) + [[F / 3**0.5] * 3], [[0, F, 0]], _forces(F), [[F, 0, 0], [0, 0, F]]]
+    p = S.Params3D(precision=prec, **PRM)
+    v = -1 if prec == "fp16" else 4 * 15 + 11
+    need = sum(S.Batch.bytes_needed(s.shape, len(f), prec) for s, f in zip(structs[:2], fsets[:2]))
+    b = S.Batch(precision=prec, hbm_budget=int(1.05 * need), chunk=16, variant=v)
+    pending = list(range(len(structs)))
+    done = {}
+    for _ in range(4000):
+        while pending and b.submit(structs[pending[0]], fsets[pending[0]], p, tag=pending[0]):
+            pending.pop(0)
+        b.run(2)
+        for tag, runs in b.poll():
+            done[tag] = runs
+        if len(done) == len(structs):
+            break
+    assert len(done) == len(structs) and not pending
+    for t, s in enumerate(structs):
+        alone, _, _ = S.solve3d(s, fsets[t], S.Params3D(precision=prec, variant=v, **PRM))
+        assert len(done[t]) == len(alone)
+        for a, m in zip(alone, done[t]):
+            assert (a.steps, a.converged) == (m.steps, m.converged), t
+            assert np.array_equal(a.q, m.q) and np.array_equal(a.se, m.se), t
