@@ -34,6 +34,9 @@ Reported (one JSON line, rank 0):
              `sustained`: the same mix at --serve-sustained of the rate served,
              every request run to completion, p50/p99 of all of them;
   large      512^3 GRF, tau 0.8, fixed steps: GLUPS and roofline per path;
+  plain64    the 64^3 FP64 single-solve configuration: time per tensor, q_x,
+             q_x / phi, k_xx, step counts and K against the reference
+             binary's row, and the reference binary on the host cores;
   batch      a sample of the 256-structure uneven-size mix, batched against
              one structure at a time in plain FP32;
   roofline   HBM roofline of the step kernels: algorithmic bytes (pore voxels
@@ -500,6 +503,7 @@ def run_ours(args, rank, world, local_rank):
     legs = world == 1
     serving = serve_trace(device, args.serve_precision, args) if legs and args.serve_seconds > 0 else None
     large = run_large_workload(args, device) if legs and args.large_steps > 0 else None
+    plain64 = run_plain64_leg(args, device) if legs and args.plain64_reps > 0 and rank == 0 else None
     batch = run_batch_workload(args, device) if legs and args.count > 0 else None
     out = None
     if rank == 0:
@@ -543,7 +547,7 @@ def run_ours(args, rank, world, local_rank):
             "speedup_vs_plain_fp32": kt / kt_p,
             "fp64_steps_per_direction": steps64,
             "reference_steps_per_direction": ref["steps"] if ref is not None else None,
-            "serving": serving, "large": large, "batch": batch,
+            "serving": serving, "large": large, "batch": batch, "plain64": plain64,
             "e2e": {"value": kt_e, "unit": "k-tensors/hr", "h2d_bytes_per_step": int(N),
                     "d2h_bytes_per_step": int(3 * 64)},
             "gpu_launches": int(head["launches"] + head["launches"] // 64 + 9 * args.steps),
@@ -619,6 +623,61 @@ def run_batch_workload(args, device=0):
                                   "max_rel_q_vs_plain_fp32": worst}
     out["speedup_vs_plain_fp32"] = {k: out["plain_fp32_per_solve"]["seconds"] / v["seconds"]
                                     for k, v in out.items() if k.startswith("batched_")}
+    return out
+
+
+PLAIN64_ROW = ROOT / "tests" / "golden" / "configs" / "plain64.csv"
+
+
+def run_plain64_leg(args, device=0):
+    """The plain single-solve configuration: the 64^3 sphere packing (r = 6,
+    phi 0.60, seed 0), FP64 (the reference's arithmetic), g = 1e-6 (--ff 4),
+    lag 1000, eps 1e-6, max 50000 and the reference's other defaults, the
+    three forcing directions the reference binary runs.  Device time per
+    tensor with CUDA events (autotuned FP64 variant, structure resident), the
+    outputs the configuration names (superficial q_x, pore mean q_x / phi,
+    k_xx) and every K_ij against the row the reference binary wrote for this
+    structure, and the reference binary on all host cores (a bounded
+    fixed-step sample scaled by its own step counts)."""
+    import torch
+    from flow_anizotropy_b200 import _lib
+    from flow_anizotropy_b200 import solver as S
+    from flow_anizotropy_b200 import structures as st
+    import hashlib
+    solid = st.plain_64(0)
+    ref = reference_row(PLAIN64_ROW)
+    if ref is not None and hashlib.sha256(np.ascontiguousarray(solid).tobytes()).hexdigest() != ref["sha256"]:
+        ref = None
+    F = 2.5e-7 * 4
+    forces = [[F, 0, 0], [0, F, 0], [0, 0, F]]
+    mu = (1.0 / 3.0) * (1.0 - 0.5)
+    phi = float((solid == 0).mean())
+    best, _ = S.tune3d(solid, ndir=3, precision="fp64", nsteps=100, device=device)
+    p = S.Params3D(precision="fp64", tau=1.0, eps=1e-6, lag=1000, max_steps=50000, variant=best)
+    dev = torch.from_numpy(np.ascontiguousarray(solid)).cuda(device)
+    ctx = _lib.context(device)
+    S.solve3d(dev, forces, p, device=device)
+    reps = max(1, args.plain64_reps)
+    with EventTimer(torch, ctx.stream) as t:
+        for _ in range(reps):
+            runs, rc, _ = S.solve3d(dev, forces, p, device=device)
+    sec = t.ms / 1e3 / reps
+    K = tensor_K(runs, mu, F)
+    out = {"workload": "64^3 sphere packing r=6 phi=0.60 seed 0, FP64, 3 directions, g=1e-6, lag 1000, eps 1e-6",
+           "kernel_variant": best, "seconds_per_tensor": sec, "k_tensors_per_hr": 3600.0 / sec,
+           "steps_per_direction": [r.steps for r in runs], "converged": [r.converged for r in runs],
+           "superficial_q_x": float(runs[0].q[0]), "pore_mean_q_x": float(runs[0].q[0] / phi),
+           "porosity": phi, "k_xx": float(K[0, 0])}
+    if ref is not None:
+        cpu = cpu_sample(solid, dict(ff=4.0, tau=1.0), seconds_target=min(args.cpu_seconds, 6.0))
+        ent = cpu_baseline_entry(cpu, solid.size, ref["steps"], f"the reference's own run ({ref['path']})")
+        out.update({"reference_steps_per_direction": ref["steps"],
+                    "steps_equal_reference": [r.steps for r in runs] == ref["steps"],
+                    "rel_err_vs_reference": k_errors(K, ref["K"]),
+                    "q_rel_err_vs_reference": float(np.abs(np.array([r.q for r in runs]) - ref["q"]).max()
+                                                    / np.abs(ref["q"]).max()),
+                    "reference_one_core_seconds_recorded": ref["seconds"],
+                    "cpu_baseline": ent})
     return out
 
 
@@ -861,6 +920,8 @@ def main():
     ap.add_argument("--group2d", type=int, default=16, help="images per launch of the perm2d workload")
     ap.add_argument("--large-n", type=int, default=512, help="cell edge of the large workload")
     ap.add_argument("--large-steps", type=int, default=2000, help="fixed steps of the large leg (0: no large leg)")
+    ap.add_argument("--plain64-reps", type=int, default=3,
+                    help="timed 64^3 FP64 single-solve tensors (the plain configuration; 0: no leg)")
     ap.add_argument("--gen-size", type=int, default=80, help="cell edge of the gen3d workload")
     ap.add_argument("--count", type=int, default=48,
                     help="structures of the batch leg / workload (0: no batch leg)")
