@@ -550,7 +550,10 @@ def run_ours(args, rank, world, local_rank):
             "serving": serving, "large": large, "batch": batch, "plain64": plain64,
             "e2e": {"value": kt_e, "unit": "k-tensors/hr", "h2d_bytes_per_step": int(N),
                     "d2h_bytes_per_step": int(3 * 64)},
-            "gpu_launches": int(head["launches"] + head["launches"] // 64 + 9 * args.steps),
+            # step launches, the deferred reduction, controller and step-base
+            # kernels of every 64-launch graph chunk, and the 8 set-up kernels
+            # of each solve (mask packing, rank tables, records, 3 lattices)
+            "gpu_launches": int(head["launches"] + 3 * (head["launches"] // 64) + 8 * args.steps),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "alg_bytes_per_launch": per_launch_alg,
