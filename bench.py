@@ -34,6 +34,9 @@ Reported (one JSON line, rank 0):
              `sustained`: the same mix at --serve-sustained of the rate served,
              every request run to completion, p50/p99 of all of them;
   large      512^3 GRF, tau 0.8, fixed steps: GLUPS and roofline per path;
+  perm2d     the D2Q9 solver (the 2D drop-in's solve) on --perm2d-images
+             seeded 256^2 disc packings with the 2D reference's defaults:
+             images/s, GLUPS, roofline, the reference binary on the host cores;
   plain64    the 64^3 FP64 single-solve configuration: time per tensor, q_x,
              q_x / phi, k_xx, step counts and K against the reference
              binary's row, and the reference binary on the host cores;
@@ -505,6 +508,11 @@ def run_ours(args, rank, world, local_rank):
     large = run_large_workload(args, device) if legs and args.large_steps > 0 else None
     plain64 = run_plain64_leg(args, device) if legs and args.plain64_reps > 0 and rank == 0 else None
     batch = run_batch_workload(args, device) if legs and args.count > 0 else None
+    perm2d = None
+    if legs and args.perm2d_images > 0 and rank == 0:
+        a2 = argparse.Namespace(**{**vars(args), "count": args.perm2d_images,
+                                   "cpu_seconds": min(args.cpu_seconds, 6.0)})
+        perm2d = run_perm2d_workload(a2, device)
     out = None
     if rank == 0:
         cpu = cpu_sample(solid, wl, seconds_target=args.cpu_seconds)
@@ -547,7 +555,7 @@ def run_ours(args, rank, world, local_rank):
             "speedup_vs_plain_fp32": kt / kt_p,
             "fp64_steps_per_direction": steps64,
             "reference_steps_per_direction": ref["steps"] if ref is not None else None,
-            "serving": serving, "large": large, "batch": batch, "plain64": plain64,
+            "serving": serving, "large": large, "batch": batch, "plain64": plain64, "perm2d": perm2d,
             "e2e": {"value": kt_e, "unit": "k-tensors/hr", "h2d_bytes_per_step": int(N),
                     "d2h_bytes_per_step": int(3 * 64)},
             # step launches, the deferred reduction, controller and step-base
@@ -923,6 +931,8 @@ def main():
     ap.add_argument("--group2d", type=int, default=16, help="images per launch of the perm2d workload")
     ap.add_argument("--large-n", type=int, default=512, help="cell edge of the large workload")
     ap.add_argument("--large-steps", type=int, default=2000, help="fixed steps of the large leg (0: no large leg)")
+    ap.add_argument("--perm2d-images", type=int, default=16,
+                    help="D2Q9 leg: seeded 256^2 images solved to convergence, both directions (0: no leg)")
     ap.add_argument("--plain64-reps", type=int, default=3,
                     help="timed 64^3 FP64 single-solve tensors (the plain configuration; 0: no leg)")
     ap.add_argument("--gen-size", type=int, default=80, help="cell edge of the gen3d workload")
