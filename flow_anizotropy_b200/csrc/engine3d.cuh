@@ -166,7 +166,12 @@ constexpr int DEFER_SLOTS = 64;
 // that other warps' gathers still need; on the 128^3 workload's access
 // pattern alone, 119 -> 83 us per 2-byte launch and 152 -> 120 us per
 // 4-byte one).  The slots within a buffer are those of the in-place form, so
-// the kernels, their arithmetic and their bits are unchanged.
+// the kernels, their arithmetic and their bits are unchanged.  In the
+// in-place form the even kernels' source and destination pointers are the
+// same lattice: every slot belongs to one (thread, voxel, link), which loads
+// it and later stores a value computed from that load, so no load and store
+// of one address are unordered by data dependence, and loads of a thread's
+// next voxel may move above its previous voxel's stores (disjoint slots).
 template <class T>
 __device__ __forceinline__ T *aa_buf(const Solve3 &S, long long m)
 {
