@@ -543,8 +543,9 @@ def run_ours(args, rank, world, local_rank):
                        "criterion": "block means, batch-means SE, k-sigma" if head_prec in ("fp16", "bf16")
                        else "drift (reference)",
                        "parallelism": f"work partition x{world} (one tensor stream per GPU)",
-                       "l2": "lattices (3 x 19 x 0.94 M pores x elem: 215 MB fp32, 108 MB fp16) stream from HBM "
-                             "every step; inputs are the whole tensor solve, not a cached kernel"},
+                       "l2": "inputs larger than L2: the lattices (3 directions x 19 planes x 0.94 M pores x "
+                             "element, two lattices in the default forms: 431 MB fp32, 216 MB 16-bit) exceed the "
+                             "126 MB L2 and stream from HBM every step; a bench step is a whole tensor solve"},
             "glups_fluid": gf, "glups_all_node": ga,
             "steps_per_direction": [r.steps for r in head["runs"]],
             "rel_err_vs_fp64": head["err"], "rel_err_vs_reference": head["err_ref"],
